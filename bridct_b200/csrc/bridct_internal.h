@@ -1,0 +1,67 @@
+// Internal types shared by the host-side translation units of libbridct_b200.so.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "plain_launch.cuh"
+
+namespace bridct {
+
+// One per CUDA device, created on first use and immutable afterwards.
+struct DeviceCtx {
+  int device = 0;
+  int sm_count = 0;
+  int major = 0, minor = 0;
+  long long l2_bytes = 0;
+  LaunchCtx launch{};
+  PlainLauncher plain[8][8][3] = {};
+  FourStepTables fourstep[4] = {};      // N = 128, 256, 512, 1024
+  std::vector<void*> table_mem;
+  FourStepTables tables(int n) const;
+};
+
+void set_error(const std::string& s);
+int cuda_fail(cudaError_t e, const char* what);
+double sj_scale(int n, int k);
+DeviceCtx* device_ctx(int device);
+int current_device(int* dev);
+const void* device_address(const void* p, bool* pinned);
+
+}  // namespace bridct
+
+struct bridct_plan {
+  int h = 0, w = 0;
+  size_t elements = 0;
+  int square = 0;
+  int device = 0;
+  bridct::DeviceCtx* dev = nullptr;
+  cudaStream_t stream = nullptr;
+  float* d_x = nullptr;        // one-array device staging
+  float* d_y = nullptr;
+  float* pin = nullptr;        // one-array pinned staging (in, out)
+  // batch pipeline (allocated on the first host-pointer batch call)
+  cudaStream_t aux[2] = {nullptr, nullptr};
+  float* d_batch = nullptr;    // 2 slots x (in, out) x chunk
+  float* pin_batch = nullptr;  // 2 slots x (in, out) x chunk, pageable callers only
+  size_t chunk = 0;            // arrays per pipeline chunk
+  // precision-form scratch (allocated on first use of a tensor-core form)
+  void* tc_mem = nullptr;
+  size_t tc_bytes = 0;
+};
+
+namespace bridct {
+int launch_plain_form(const bridct_plan* p, int mode, const float* x, float* y, long long batch,
+                      cudaStream_t st);
+int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, size_t batch,
+                        const float* dx, float* dy, bool pin_in, bool pin_out);
+bridct_plan* thread_square_plan(int n);
+void release_plan_extras(bridct_plan* p);
+}  // namespace bridct
+
+namespace bridct {
+// Tensor-core precision forms (tc_forms.cu).
+int apply_tc_form(bridct_plan* p, int mode, int form, const float* x, float* y, size_t batch,
+                  void* stream);
+}  // namespace bridct

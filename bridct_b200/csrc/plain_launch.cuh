@@ -1,0 +1,74 @@
+// Host-side launch logic of the plain form for one compile-time shape (H, W) and mode.
+#pragma once
+#include <cuda_runtime.h>
+#include "sj_kernels.cuh"
+
+namespace bridct {
+
+struct LaunchCtx {
+  int sm_count;
+  long long l2_chunk_bytes;   // working-set budget of one column+row pass pair
+};
+
+using PlainLauncher = cudaError_t (*)(const float*, float*, long long, cudaStream_t,
+                                      LineTables, const LaunchCtx&);
+
+// Blocks per SM for a kernel at a given dynamic shared-memory size (computed once).
+template <typename Kernel>
+static int kernel_blocks_per_sm(Kernel k, int smem) {
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return 0;
+  }
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kThreads, smem) != cudaSuccess) return 0;
+  return b;
+}
+
+template <typename Kernel>
+static cudaError_t launch_tiles(Kernel k, int smem, int bps, TileArgs a, const LaunchCtx& ctx,
+                                cudaStream_t st) {
+  if (bps <= 0) return cudaErrorInvalidConfiguration;
+  if (a.ntiles <= 0) return cudaSuccess;
+  long long grid = (long long)ctx.sm_count * bps;
+  if (grid > a.ntiles) grid = a.ntiles;
+  k<<<(unsigned)grid, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int H, int W, int MODE>
+cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t st,
+                         LineTables tab, const LaunchCtx& ctx) {
+  using Gm = Geometry<H, W>;
+  if (batch <= 0) return cudaSuccess;
+  if constexpr (Gm::kTile) {
+    auto k = k_full<H, W, Gm::kTR, true, true, MODE>;
+    static const int bps = kernel_blocks_per_sm(k, Gm::kSmemFull);
+    TileArgs a{x, y, (batch * H + Gm::kTR - 1) / Gm::kTR, batch * H, tab};
+    return launch_tiles(k, Gm::kSmemFull, bps, a, ctx, st);
+  } else {
+    auto kc = k_colstrip<H, W, Gm::kTC, MODE>;
+    auto kr = k_full<H, W, Gm::kRB, false, true, MODE>;
+    static const int bpc = kernel_blocks_per_sm(kc, Gm::kSmemStrip);
+    static const int bpr = kernel_blocks_per_sm(kr, Gm::kSmemRows);
+    const long long bytes = (long long)H * W * 4;
+    long long chunk = ctx.l2_chunk_bytes / bytes;
+    if (chunk < 1) chunk = 1;
+    for (long long b0 = 0; b0 < batch; b0 += chunk) {
+      const long long nb = batch - b0 < chunk ? batch - b0 : chunk;
+      const long long off = b0 * H * W;
+      TileArgs ac{x + off, y + off, nb * (W / Gm::kTC), nb * H, tab};
+      cudaError_t e = launch_tiles(kc, Gm::kSmemStrip, bpc, ac, ctx, st);
+      if (e != cudaSuccess) return e;
+      TileArgs ar{y + off, y + off, nb * H / Gm::kRB, nb * H, tab};
+      e = launch_tiles(kr, Gm::kSmemRows, bpr, ar, ctx, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+}
+
+// Per-H instantiation units (plain_inst.cu compiled once per H) export this table row.
+void plain_table_row(int h, PlainLauncher (*row)[3]);
+
+}  // namespace bridct

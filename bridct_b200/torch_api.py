@@ -1,0 +1,145 @@
+"""PyTorch entry point for CUDA tensors (the reference has none; it mirrors the `Plan`
+semantics of the NumPy entry for device-resident data).
+
+    y = bridct_b200.torch_api.dct2(x)          # x: (..., H, W) float32 CUDA tensor
+    x = bridct_b200.torch_api.idct2(y)
+    z = bridct_b200.torch_api.roundtrip2(x)
+
+The calls are asynchronous on torch's current CUDA stream and run the plain Shao-Johnson
+kernels, or a tensor-core precision form with ``form="tc_bf16x3" | "tc_tf32x3" | "tc_fp8"``.
+`dct2`/`idct2` are differentiable: the transforms are orthonormal and linear, so the
+gradient of the DCT-II is the DCT-III of the incoming gradient and vice versa.
+"""
+from __future__ import annotations
+
+import threading
+from typing import Dict, Tuple
+
+import torch
+
+from . import _lib
+
+_FORMS = {"sj": _lib.FORM_SJ, "tc_bf16x3": _lib.FORM_TC_BF16X3, "tc_tf32x3": _lib.FORM_TC_TF32X3,
+          "tc_fp8": _lib.FORM_TC_FP8}
+_plans: Dict[Tuple[int, int, int], int] = {}
+_plans_lock = threading.Lock()
+
+
+def _plan(device: int, h: int, w: int) -> int:
+    key = (device, h, w)
+    p = _plans.get(key)
+    if p:
+        return p
+    with _plans_lock:
+        p = _plans.get(key)
+        if p:
+            return p
+        with torch.cuda.device(device):
+            p = _lib.lib().bridct_plan_create(h, w)
+        if not p:
+            raise RuntimeError(f"bridct_plan_create({h}, {w}) failed: {_lib.last_error()}")
+        _plans[key] = p
+        return p
+
+
+def _check(x: torch.Tensor) -> Tuple[int, int, int]:
+    if not isinstance(x, torch.Tensor):
+        raise TypeError("Expected a torch.Tensor.")
+    if not x.is_cuda:
+        raise ValueError("Expected a CUDA tensor; use bridct_b200.bridct_numpy for host arrays.")
+    if x.dtype != torch.float32:
+        raise TypeError("Expected float32.")
+    if x.dim() < 2:
+        raise ValueError("Expected (..., height, width).")
+    h, w = x.shape[-2], x.shape[-1]
+    if not _lib.lib().bridct_supported(h, w):
+        raise ValueError("Both dimensions must be powers of two from 8 through 1024.")
+    batch = x.numel() // (h * w)
+    return h, w, batch
+
+
+def apply(x: torch.Tensor, mode: int, out: torch.Tensor = None, form: str = "sj") -> torch.Tensor:
+    """Transforms the last two axes of a CUDA float32 tensor (no autograd)."""
+    h, w, batch = _check(x)
+    if form not in _FORMS:
+        raise ValueError(f"unknown form {form!r}; expected one of {sorted(_FORMS)}")
+    x = x.contiguous()
+    if x.data_ptr() % 16:
+        x = x.clone()
+    if out is None:
+        out = torch.empty_like(x)
+    else:
+        if out.shape != x.shape or out.dtype != torch.float32 or out.device != x.device:
+            raise ValueError("Input and output shapes must match exactly.")
+        if not out.is_contiguous() or out.data_ptr() % 16:
+            raise ValueError("Expected a contiguous, 16-byte aligned output.")
+    if batch == 0:
+        return out
+    dev = x.device.index if x.device.index is not None else torch.cuda.current_device()
+    plan = _plan(dev, h, w)
+    stream = torch.cuda.current_stream(x.device).cuda_stream
+    st = _lib.lib().bridct_plan_apply_form_device(plan, mode, _FORMS[form], x.data_ptr(), out.data_ptr(),
+                                                  batch, stream)
+    _lib.check(st, "bridct_plan_apply_form_device")
+    return out
+
+
+class _DCT2(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, form):
+        ctx.form = form
+        return apply(x, _lib.FORWARD, form=form)
+
+    @staticmethod
+    def backward(ctx, g):
+        return apply(g.contiguous(), _lib.INVERSE, form=ctx.form), None
+
+
+class _IDCT2(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, form):
+        ctx.form = form
+        return apply(x, _lib.INVERSE, form=form)
+
+    @staticmethod
+    def backward(ctx, g):
+        return apply(g.contiguous(), _lib.FORWARD, form=ctx.form), None
+
+
+def dct2(x: torch.Tensor, form: str = "sj") -> torch.Tensor:
+    """Orthonormal 2D DCT-II over the last two axes (differentiable)."""
+    return _DCT2.apply(x, form)
+
+
+def idct2(x: torch.Tensor, form: str = "sj") -> torch.Tensor:
+    """Orthonormal 2D DCT-III over the last two axes (differentiable)."""
+    return _IDCT2.apply(x, form)
+
+
+def roundtrip2(x: torch.Tensor) -> torch.Tensor:
+    """Normalized round trip DCT-III(DCT-II(x)) in one pass per axis."""
+    return apply(x, _lib.ROUNDTRIP)
+
+
+class Plan:
+    """Torch counterpart of bridct_numpy.Plan for CUDA tensors of one (height, width)."""
+
+    def __init__(self, height: int, width: int, form: str = "sj"):
+        if not _lib.lib().bridct_supported(height, width):
+            raise ValueError("Both dimensions must be powers of two from 8 through 1024.")
+        self.shape = (height, width)
+        self.form = form
+
+    def _go(self, x, mode, out):
+        if tuple(x.shape[-2:]) != self.shape:
+            raise ValueError("Expected (..., height, width) matching the plan.")
+        return apply(x, mode, out=out, form=self.form if mode != _lib.ROUNDTRIP else "sj")
+
+    def forward(self, x, *, out=None):
+        return self._go(x, _lib.FORWARD, out)
+
+    def inverse(self, x, *, out=None):
+        return self._go(x, _lib.INVERSE, out)
+
+    def roundtrip(self, x, *, out=None):
+        return self._go(x, _lib.ROUNDTRIP, out)

@@ -1,0 +1,58 @@
+/* B200 extensions of the BRiDCT plan API (libbridct_b200.so).
+ *
+ * The reference has no counterpart for these entry points: it transforms one host array
+ * per call (include/bridct.h:44-45).  They let callers keep data in HBM, batch thousands of
+ * arrays per launch, choose the tensor-core precision forms, and run mixed-shape (ragged)
+ * batches in one persistent launch.  All return the status codes of bridct.h.
+ */
+#ifndef BRIDCT_B200_H
+#define BRIDCT_B200_H
+
+#include "bridct.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Execution form of a transform. */
+enum bridct_form {
+    BRIDCT_FORM_SJ = 0,        /* FP32 Shao-Johnson CUDA-core kernels (the plan API's form) */
+    BRIDCT_FORM_TC_BF16X3 = 1, /* tensor cores: 3-term bf16 split of X, 6 products, FP32 acc. */
+    BRIDCT_FORM_TC_TF32X3 = 2, /* tensor cores: 2-term tf32 split of X and C, 3 products     */
+    BRIDCT_FORM_TC_FP8 = 3     /* FP8 E4M3, per-32x32-tile scale, + one FP32 refinement step */
+};
+
+/* Thread-local description of the last failure in this thread ("" if none). */
+BRIDCT_API const char *bridct_last_error(void);
+
+/* GPU schedule of the plan: "sj-tile" (both passes in shared memory) or
+ * "sj-two-pass" (column pass then row pass through L2).  NULL for a NULL plan. */
+BRIDCT_API const char *bridct_plan_gpu_route(const bridct_plan *plan);
+
+/* `batch` contiguous h*w arrays; host (pageable or pinned) or device pointers.
+ * Synchronous.  Host buffers are streamed through the plan's device staging in
+ * chunks (H2D, kernel, D2H overlapped on two streams); the first host-pointer call
+ * allocates that staging.  Overlap of the two batch ranges -> OVERLAPPING_BUFFERS. */
+BRIDCT_API int bridct_plan_apply_batch(bridct_plan *plan, enum bridct_mode mode,
+                                       const float *input, float *output, size_t batch);
+
+/* Device-resident batch: input/output are CUDA device (or managed) pointers to
+ * batch*h*w floats, 16-byte aligned.  Asynchronous on `stream` (a cudaStream_t; NULL
+ * selects the plan's own stream).  No allocation, no host synchronisation. */
+BRIDCT_API int bridct_plan_apply_device(bridct_plan *plan, enum bridct_mode mode,
+                                        const float *input, float *output, size_t batch,
+                                        void *stream);
+
+/* As bridct_plan_apply_device, with an explicit execution form (precision forms run
+ * on the tensor cores; see enum bridct_form for the shapes each form supports). */
+BRIDCT_API int bridct_plan_apply_form_device(bridct_plan *plan, enum bridct_mode mode,
+                                             enum bridct_form form, const float *input,
+                                             float *output, size_t batch, void *stream);
+
+/* Waits for all work queued on the plan's own stream. */
+BRIDCT_API int bridct_plan_synchronize(bridct_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
