@@ -1,0 +1,432 @@
+"""Benchmark: batched 2D DCT-II GB/s on B200, plain Shao-Johnson FP32 kernels vs the
+tensor-core split-precision forms, with the reference's own CPU path timed on the host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload blocks8|arrays64|large1024|ragged|sweep256] [--form auto|sj|...]
+
+Default workload: 262,144 independent 8x8 blocks of a 4096x4096 image (pixels uniform integers
+0..255 minus 128, seed 1), forward DCT-II, blocks stored contiguously as (B, 8, 8).  A step is
+one forward transform of all blocks (one pass of the hot path over the batch).  Algorithmic
+traffic is 8 bytes per element (read 4, write 4).  Timed steps replay a CUDA graph of
+launches over 4 rotating input/output buffer sets (512 MiB, larger than the 126 MB L2), timed
+with CUDA events on the launching stream; multi-GPU runs are independent replicas per GPU
+(the batch shards with no exchange step), timed as the max over ranks.
+
+`e2e` is the same metric through the public C-ABI (bridct_plan_apply_batch) from pinned host
+buffers: every step copies the inputs host->device and the results device->host.
+`--impl reference` times the reference library (compiled from its sources into oracle/_ref)
+on the host cores with one plan per thread.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+HBM_FALLBACK = 6650.0  # GB/s, used only when MEASURED_PEAKS.json is absent
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"],
+                "bf16_tflops_sustained": d.get("bf16_tflops_sustained"), "source": "measured"}
+    return {"hbm_gbs": HBM_FALLBACK, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
+
+
+# ----------------------------------------------------------------------------------------
+# Workloads (seeded synthetic inputs with the configurations' shapes and distributions)
+# ----------------------------------------------------------------------------------------
+
+def workload(name: str):
+    if name == "blocks8":
+        img = (np.random.default_rng(1).integers(0, 256, (4096, 4096)) - 128).astype(np.float32)
+        x = img.reshape(512, 8, 512, 8).transpose(0, 2, 1, 3).reshape(-1, 8, 8).copy()
+        return dict(x=x, mode=0, desc="262,144 independent 8x8 blocks of a 4096x4096 image "
+                    "(U{0..255}-128, seed 1), forward DCT-II, contiguous (B,8,8)")
+    if name == "arrays64":
+        x = np.random.default_rng(0).uniform(-1, 1, (1024, 64, 64)).astype(np.float32)
+        return dict(x=x, mode=0, desc="1024 arrays 64x64 U[-1,1] (seed 0), forward DCT-II")
+    if name == "large1024":
+        rng = np.random.default_rng(2)
+        yy, xx = np.mgrid[0:1024, 0:1024]
+        x = (rng.standard_normal((1024, 1024)) + np.sin(2 * np.pi * xx / 97) * np.cos(2 * np.pi * yy / 61))
+        return dict(x=x.astype(np.float32)[None], mode=0, desc="one 1024x1024 N(0,1)+smooth (seed 2), forward")
+    if name == "sweep256":
+        rng = np.random.default_rng(4)
+        mag = 10.0 ** rng.uniform(-6, 6, (2048, 256, 256))
+        x = (mag * rng.choice([-1.0, 1.0], size=mag.shape)).astype(np.float32)
+        return dict(x=x, mode=0, desc="2048 arrays 256x256 log-uniform 1e-6..1e6 (seed 4), forward")
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ----------------------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ----------------------------------------------------------------------------------------
+
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [v.strip() for v in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------------
+# Reference CPU path
+# ----------------------------------------------------------------------------------------
+
+def _ref_call(x, mode, n, threads, repeats):
+    from oracle import oracle as O
+
+    b, h, w = x.shape
+    y = np.empty_like(x)
+    hs = np.full(n, h, np.int32)
+    ws = np.full(n, w, np.int32)
+    modes = np.full(n, mode, np.int32)
+    offs = np.arange(n, dtype=np.uint64) * np.uint64(h * w)
+    return O.ref_bench(hs, ws, modes, offs, x, y, threads, repeats)
+
+
+def ref_sample_size(x, mode, threads, seconds_per_pass):
+    """Arrays per pass so that one pass over them takes about `seconds_per_pass`."""
+    b = x.shape[0]
+    n0 = min(b, 64 * threads)
+    t0 = _ref_call(x, mode, n0, threads, 3) / 3
+    return int(min(b, max(threads, n0 * seconds_per_pass / max(t0, 1e-9))))
+
+
+def cpu_reference(x: np.ndarray, mode: int, threads: int, budget_s: float):
+    """Times the reference library on `threads` host cores; returns (GB/s, sample text)."""
+    from oracle import oracle as O
+
+    if not O.bench_available():
+        return None, "reference library not built (oracle/_ref missing)"
+    b, h, w = x.shape
+    n = ref_sample_size(x, mode, threads, 0.25)
+    t1 = _ref_call(x, mode, n, threads, 1)
+    reps = max(1, int(budget_s / max(t1, 1e-9)))
+    t = _ref_call(x, mode, n, threads, reps)
+    gbs = 8.0 * h * w * n * reps / t / 1e9
+    return gbs, f"{n} of {b} arrays x {reps} passes ({t:.2f} s, {threads} threads, one plan per thread)"
+
+
+def run_reference_arm(args, rank: int, world: int):
+    from oracle import oracle as O
+
+    if rank != 0:
+        return
+    wl = workload(args.workload)
+    x = wl["x"]
+    b, h, w = x.shape
+    threads = O.host_threads()
+    line = {"metric": METRIC, "unit": "GB/s", "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl["desc"], "arrays": b, "shape": [h, w], "mode": "forward"}}
+    if not O.bench_available():
+        line["unavailable"] = "reference library not built (oracle/_ref missing)"
+        print(json.dumps(line))
+        return
+    # Each step is one pass over a bounded sample of the workload on all host threads,
+    # sized so that warm-up plus timed steps stay within about a minute.
+    per_step = min(0.5, 60.0 / max(1, args.steps + args.warmup))
+    n = ref_sample_size(x, wl["mode"], threads, per_step)
+    if args.warmup:
+        _ref_call(x, wl["mode"], n, threads, args.warmup)
+    total = _ref_call(x, wl["mode"], n, threads, args.steps)
+    gbs = 8.0 * h * w * n * args.steps / total / 1e9
+    line.update(value=gbs, ms_per_step=1e3 * total / args.steps)
+    line["config"]["sample_arrays_per_step"] = n
+    line["cpu_baseline"] = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "reference",
+                            "sample": f"{n} of {b} arrays per step, {threads} threads, one plan per thread"}
+    line["e2e"] = {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    print(json.dumps(line))
+
+
+# ----------------------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------------------
+
+METRIC = "batched 2D DCT-II GB/s (% HBM peak): TC split-prec vs FP32 SJ at equal error"
+
+
+def time_form(torch, lib, plan, form_id, xs, ys, batch, mode, steps, warmup, stream):
+    """Device time (ms) of `steps` launches replayed from CUDA graphs over rotating buffers."""
+    sets = len(xs)
+
+    def launch(i):
+        st = lib.bridct_plan_apply_form_device(plan, mode, form_id, xs[i % sets].data_ptr(),
+                                               ys[i % sets].data_ptr(), batch, stream.cuda_stream)
+        if st != 0:
+            raise RuntimeError(f"launch failed: {st}")
+
+    with torch.cuda.stream(stream):
+        for i in range(max(3, warmup)):
+            launch(i)
+    stream.synchronize()
+    chunk = min(steps, 256)
+    graphs = []
+    for n in sorted({chunk, steps % chunk} - {0}, reverse=True):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            for i in range(n):
+                launch(i)
+        graphs.append((n, g))
+    stream.synchronize()
+    plan_of = []
+    left = steps
+    while left >= chunk:
+        plan_of.append(graphs[0][1])
+        left -= chunk
+    if left:
+        plan_of.append([g for n, g in graphs if n == left][0])
+    with torch.cuda.stream(stream):
+        graphs[0][1].replay()   # warm the graph path
+    stream.synchronize()
+    return plan_of
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="blocks8")
+    ap.add_argument("--form", default="auto")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus))
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    if args.impl == "reference":
+        if world > 1:
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=300))
+        run_reference_arm(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from bridct_b200 import _lib, torch_api
+    from oracle import oracle as O
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    lib = _lib.lib()
+    wl = workload(args.workload)
+    xh = wl["x"]
+    b, h, w = xh.shape
+    mode = wl["mode"]
+    bytes_step = 8.0 * b * h * w
+    sets = max(1, int(np.ceil(2 * 126e6 / (2 * 4 * b * h * w)))) if b * h * w * 8 < 2 * 126e6 else 1
+    sets = max(sets, 2)
+    dev = torch.device("cuda", local)
+    xd = torch.from_numpy(xh).to(dev)
+    xs = [xd.clone() for _ in range(sets)]
+    ys = [torch.empty_like(xd) for _ in range(sets)]
+    plan = torch_api._plan(local, h, w)
+    stream = torch.cuda.Stream(device=dev)
+
+    forms = {"sj": _lib.FORM_SJ}
+    if args.form in ("auto",):
+        for name, fid in (("tc_bf16x3", _lib.FORM_TC_BF16X3), ("tc_tf32x3", _lib.FORM_TC_TF32X3)):
+            probe = lib.bridct_plan_apply_form_device(plan, mode, fid, xs[0].data_ptr(), ys[0].data_ptr(), b,
+                                                      stream.cuda_stream)
+            if probe == 0:
+                forms[name] = fid
+        stream.synchronize()
+    elif args.form != "sj":
+        forms = {args.form: {"tc_bf16x3": _lib.FORM_TC_BF16X3, "tc_tf32x3": _lib.FORM_TC_TF32X3,
+                             "tc_fp8": _lib.FORM_TC_FP8}[args.form]}
+
+    # accuracy of each form on a sample, against float64 (equal-error comparison)
+    sample = slice(0, min(b, 4096 if h * w <= 4096 else 8))
+    xs_np = xh[sample]
+    exact = O.fp64_apply(xs_np, mode)
+    results = {}
+    for name, fid in forms.items():
+        st = lib.bridct_plan_apply_form_device(plan, mode, fid, xs[0].data_ptr(), ys[0].data_ptr(), b,
+                                               stream.cuda_stream)
+        stream.synchronize()
+        yv = ys[0].cpu().numpy()[sample]
+        results[name] = {"max_rel_err": O.rel_max_error(yv, exact, xs_np),
+                         "max_rel_err_output_scaled": O.rel_max_error(yv, exact, xs_np, output_scaled=True),
+                         "rms_rel_err": O.rel_rms_error(yv, exact, xs_np), "status": st}
+
+    timings = {}
+    for name, fid in forms.items():
+        graphs = time_form(torch, lib, plan, fid, xs, ys, b, mode, args.steps, args.warmup, stream)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        clk = Clocks(local)
+        with clk:
+            with torch.cuda.stream(stream):
+                start.record(stream)
+                for g in graphs:
+                    g.replay()
+                end.record(stream)
+            end.synchronize()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = start.elapsed_time(end)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        timings[name] = {"ms_total": ms, "ms_per_step": ms / args.steps, "clocks": clk.summary(),
+                         "gbs": bytes_step * args.steps * world / (ms * 1e-3) / 1e9}
+        del graphs
+
+    # headline: the fastest form whose error meets the bound (2e-6, output-scaled max norm)
+    ok = [n for n in timings if results[n]["max_rel_err_output_scaled"] <= 2e-6]
+    head = max(ok or list(timings), key=lambda n: timings[n]["gbs"])
+    pk = peaks()
+    per_launch_s = timings[head]["ms_per_step"] * 1e-3
+    achieved = bytes_step / per_launch_s / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(f"{args.workload}:{head}")
+
+    # e2e through the public C-ABI with pinned host buffers
+    hin = torch.from_numpy(xh).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    e2e_steps = max(3, min(50, args.steps))
+    for _ in range(2):
+        _lib.check(lib.bridct_plan_apply_batch(plan, mode, hin.data_ptr(), hout.data_ptr(), b))
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        _lib.check(lib.bridct_plan_apply_batch(plan, mode, hin.data_ptr(), hout.data_ptr(), b))
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": bytes_step * e2e_steps * world / e2e_s / 1e9, "unit": "GB/s",
+           "h2d_bytes_per_step": int(4 * b * h * w), "d2h_bytes_per_step": int(4 * b * h * w),
+           "form": "sj", "ms_per_step": 1e3 * e2e_s / e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = O.host_threads()
+        gbs, sample_txt = cpu_reference(xh, mode, threads, budget_s=2.0)
+        if gbs is not None:
+            cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "reference", "sample": sample_txt}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC,
+        "value": timings[head]["gbs"],
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": timings[head]["ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if head == "sj" else head.replace("tc_", "") + "/f32-acc",
+        "data": "synthetic",
+        "config": {"workload": wl["desc"], "arrays": b, "shape": [h, w], "mode": "forward",
+                   "form": head, "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": f"{sets} rotating input/output sets ({sets * 8 * b * h * w / 2**20:.0f} MiB) > L2",
+                   "timing": "CUDA events on the launch stream around CUDA-graph replays"},
+        "pct_hbm_peak": 100.0 * achieved / pk["hbm_gbs"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"],
+                     "traffic": traffic, "algorithmic_bytes_per_launch": bytes_step},
+        "forms": {n: {**results[n], "gbs": timings[n]["gbs"], "ms_per_step": timings[n]["ms_per_step"],
+                      "pct_hbm": 100 * timings[n]["gbs"] / world / pk["hbm_gbs"]} for n in timings},
+        "clocks": timings[head]["clocks"],
+        "e2e": e2e,
+        "gpu_launches": int(args.steps * launches_per_step(h, w, b)),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+def launches_per_step(h: int, w: int, b: int) -> int:
+    if h * w <= 16384:
+        return 1
+    chunk = max(1, (126 * 2**20 // 4) // (4 * h * w))
+    return 2 * int(np.ceil(b / chunk))
+
+
+if __name__ == "__main__":
+    main()

@@ -324,8 +324,8 @@ BRIDCT_API int bridct_plan_apply_device(bridct_plan* plan, enum bridct_mode mode
   const size_t bytes = plan->elements * sizeof(float) * batch;
   if (ranges_overlap((uintptr_t)input, bytes, (uintptr_t)output, bytes)) return BRIDCT_OVERLAPPING_BUFFERS;
   if (((uintptr_t)input | (uintptr_t)output) % 16) return BRIDCT_BAD_ALIGNMENT;
-  cudaStream_t st = stream ? (cudaStream_t)stream : plan->stream;
-  return launch_plain_form(plan, mode, input, output, (long long)batch, st);
+  // NULL is the CUDA default stream, as everywhere in CUDA (torch's default stream too).
+  return launch_plain_form(plan, mode, input, output, (long long)batch, (cudaStream_t)stream);
 }
 
 BRIDCT_API int bridct_plan_synchronize(bridct_plan* plan) {

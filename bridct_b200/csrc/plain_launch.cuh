@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "sj_kernels.cuh"
+#include "sj_blocks8.cuh"
 
 namespace bridct {
 
@@ -41,7 +42,17 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
                          LineTables tab, const LaunchCtx& ctx) {
   using Gm = Geometry<H, W>;
   if (batch <= 0) return cudaSuccess;
-  if constexpr (Gm::kTile) {
+  if constexpr (H == 8 && W == 8) {
+    auto k = k_blocks8<MODE>;
+    constexpr int smem = kB8Chunks * 16;
+    static const int bps = kernel_blocks_per_sm(k, smem);
+    if (bps <= 0) return cudaErrorInvalidConfiguration;
+    const long long ntiles = (batch + kB8Threads - 1) / kB8Threads;
+    long long grid = (long long)ctx.sm_count * bps;
+    if (grid > ntiles) grid = ntiles;
+    k<<<(unsigned)grid, kB8Threads, smem, st>>>(x, y, batch);
+    return cudaGetLastError();
+  } else if constexpr (Gm::kTile) {
     auto k = k_full<H, W, Gm::kTR, true, true, MODE>;
     static const int bps = kernel_blocks_per_sm(k, Gm::kSmemFull);
     TileArgs a{x, y, (batch * H + Gm::kTR - 1) / Gm::kTR, batch * H, tab};

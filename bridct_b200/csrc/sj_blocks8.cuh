@@ -1,0 +1,91 @@
+// 8x8 arrays (the block-transform batch): one thread owns one whole 8x8 array in registers
+// and runs 8 row lines and 8 column lines of the generated SJ 8-point program; the CTA
+// stages its tile of 256 arrays through shared memory so that global loads and stores are
+// fully coalesced 16-byte accesses.
+//
+// Shared-memory layout: array b occupies 256 bytes = sixteen 16-byte chunks; chunk j of array
+// b is stored at chunk position (j ^ (b & 15)).  A thread reading chunk j of its own array and
+// seven neighbours reading chunk j of theirs (one 8-thread phase of a 128-bit access) then hit
+// eight distinct 16-byte bank groups, so every shared-memory access is conflict free; the
+// coalesced tile copy (consecutive threads, consecutive chunks of one array) is conflict free
+// for the same reason.
+#pragma once
+#include "sj_lines.cuh"
+
+namespace bridct {
+
+constexpr int kB8Threads = 256;            // arrays per tile = threads per CTA
+constexpr int kB8Chunks = kB8Threads * 16; // 16-byte chunks per tile
+
+__device__ __forceinline__ int b8_slot(int chunk) {
+  const int b = chunk >> 4, j = chunk & 15;
+  return (b << 4) | (j ^ (b & 15));
+}
+
+template <int MODE>
+__device__ __forceinline__ void b8_transform(float (&v)[64]) {
+  // rows (contiguous 8-float lines)
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    float t[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) t[c] = v[r * 8 + c];
+    reg_line_apply<8, MODE>(t);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) v[r * 8 + c] = t[c];
+  }
+  // columns
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    float t[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) t[r] = v[r * 8 + c];
+    reg_line_apply<8, MODE>(t);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r * 8 + c] = t[r];
+  }
+}
+
+// x, y: `batch` contiguous 8x8 arrays (16-byte aligned).
+template <int MODE>
+__global__ void __launch_bounds__(kB8Threads) k_blocks8(const float* __restrict__ x,
+                                                        float* __restrict__ y, long long batch) {
+  extern __shared__ float4 s8[];
+  const long long ntiles = (batch + kB8Threads - 1) / kB8Threads;
+  const int t = threadIdx.x;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long first = tile * kB8Threads;
+    const int arrays = batch - first < kB8Threads ? (int)(batch - first) : kB8Threads;
+    const int chunks = arrays * 16;
+    const float4* src = reinterpret_cast<const float4*>(x) + first * 16;
+    float4 buf[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int q = t + k * kB8Threads;
+      buf[k] = q < chunks ? __ldg(src + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s8[b8_slot(t + k * kB8Threads)] = buf[k];
+    __syncthreads();
+    float v[64];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const float4 c = s8[b8_slot(t * 16 + j)];
+      v[4 * j] = c.x; v[4 * j + 1] = c.y; v[4 * j + 2] = c.z; v[4 * j + 3] = c.w;
+    }
+    b8_transform<MODE>(v);
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      s8[b8_slot(t * 16 + j)] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+    __syncthreads();
+    float4* dst = reinterpret_cast<float4*>(y) + first * 16;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int q = t + k * kB8Threads;
+      if (q < chunks) dst[q] = s8[b8_slot(q)];
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace bridct

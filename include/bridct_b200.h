@@ -38,7 +38,7 @@ BRIDCT_API int bridct_plan_apply_batch(bridct_plan *plan, enum bridct_mode mode,
 
 /* Device-resident batch: input/output are CUDA device (or managed) pointers to
  * batch*h*w floats, 16-byte aligned.  Asynchronous on `stream` (a cudaStream_t; NULL
- * selects the plan's own stream).  No allocation, no host synchronisation. */
+ * is the CUDA default stream).  No allocation, no host synchronisation. */
 BRIDCT_API int bridct_plan_apply_device(bridct_plan *plan, enum bridct_mode mode,
                                         const float *input, float *output, size_t batch,
                                         void *stream);
