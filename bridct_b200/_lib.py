@@ -66,6 +66,7 @@ EXTRA_SIGNATURES = [
     ("bridct_ragged_apply_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("bridct_ragged_apply_loop_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("bridct_ragged_route", C.c_char_p, [C.c_void_p]),
+    ("bridct_device_timeout_flag", C.c_int, [C.c_int]),
 ]
 
 

@@ -49,6 +49,10 @@ BRIDCT_API int bridct_plan_apply_form_device(bridct_plan *plan, enum bridct_mode
                                              enum bridct_form form, const float *input,
                                              float *output, size_t batch, void *stream);
 
+/* Reads and clears the bounded-wait flag of a device: nonzero when a tensor-core kernel's
+ * mbarrier wait expired (the kernel then skipped its remaining tiles and returned). */
+BRIDCT_API int bridct_device_timeout_flag(int device);
+
 /* Waits for all work queued on the plan's own stream. */
 BRIDCT_API int bridct_plan_synchronize(bridct_plan *plan);
 

@@ -1,0 +1,75 @@
+"""Tensor-core precision forms (tcgen05/TMEM/TMA) for 8x8 batches against float64.
+
+Tolerance: max|y - y64| / max(max|x|, max|y64|) <= 2e-6 per array, the same bound as the
+plain form; the literal max|x| form of the bound is checked on the block-image data.
+"""
+import numpy as np
+import pytest
+import torch
+
+from bridct_b200 import _lib, torch_api
+from oracle import oracle as O
+from tests.helpers import TOL
+
+pytestmark = pytest.mark.gpu
+
+FORMS = ["tc_bf16x3", "tc_tf32x3"]
+
+
+def run(x: np.ndarray, mode: int, form: str) -> np.ndarray:
+    t = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    y = torch_api.apply(t, mode, form=form)
+    torch.cuda.synchronize()
+    assert _lib.lib().bridct_device_timeout_flag(torch.cuda.current_device()) == 0
+    return y.cpu().numpy()
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("batch", [1, 127, 128, 300, 4096])
+def test_tc8_matches_fp64(form, batch):
+    x = np.random.default_rng(batch).uniform(-1, 1, (batch, 8, 8)).astype(np.float32)
+    for mode in range(3):
+        y = run(x, mode, form)
+        assert O.rel_max_error(y, O.fp64_apply(x, mode), x, output_scaled=True) <= TOL, (form, batch, mode)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_tc8_block_image_literal_bound(form):
+    img = (np.random.default_rng(1).integers(0, 256, (1024, 1024)) - 128).astype(np.float32)
+    x = img.reshape(128, 8, 128, 8).transpose(0, 2, 1, 3).reshape(-1, 8, 8).copy()
+    y = run(x, 0, form)
+    exact = O.fp64_apply(x, 0)
+    assert O.rel_max_error(y, exact, x) <= TOL
+    assert O.rel_rms_error(y, exact, x) <= TOL / 4
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_tc8_extreme_magnitudes(form):
+    rng = np.random.default_rng(4)
+    mag = 10.0 ** rng.uniform(-6, 6, (512, 1, 1))
+    x = (mag * rng.uniform(-1, 1, (512, 8, 8))).astype(np.float32)
+    for mode in range(2):
+        y = run(x, mode, form)
+        assert O.rel_max_error(y, O.fp64_apply(x, mode), x, output_scaled=True) <= TOL
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_tc8_no_write_past_batch(form):
+    L = _lib.lib()
+    plan = torch_api._plan(torch.cuda.current_device(), 8, 8)
+    x = torch.randn(301, 8, 8, device="cuda")
+    y = torch.full_like(x, 12345.0)
+    fid = {"tc_bf16x3": _lib.FORM_TC_BF16X3, "tc_tf32x3": _lib.FORM_TC_TF32X3}[form]
+    assert L.bridct_plan_apply_form_device(plan, 0, fid, x.data_ptr(), y.data_ptr(), 300, None) == 0
+    torch.cuda.synchronize()
+    assert (y[300] == 12345.0).all()
+    assert torch.isfinite(y[:300]).all()
+
+
+def test_tc_forms_reject_other_shapes():
+    L = _lib.lib()
+    plan = torch_api._plan(torch.cuda.current_device(), 16, 16)
+    x = torch.randn(4, 16, 16, device="cuda")
+    y = torch.empty_like(x)
+    st = L.bridct_plan_apply_form_device(plan, 0, _lib.FORM_TC_BF16X3, x.data_ptr(), y.data_ptr(), 4, None)
+    assert st == _lib.INVALID_ARGUMENT
