@@ -12,15 +12,17 @@
 // K and its splits are computed in float64 on the host and uploaded once, already in the
 // shared-memory image the MMA reads (128-byte swizzled, K-major).
 //
-// Per tile: one elected thread starts a TMA load of the FP32 tile (two 128x32 boxes, 128-byte
-// swizzle, exactly the UMMA K-major SW128 layout), the 128 threads split it into the operand
-// tiles, one thread issues the MMAs and commits them to an mbarrier, the 4 warps read the
-// accumulator back with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile rows), write it
-// swizzled to shared memory and one thread TMA-stores the tile.  Two CTAs per SM overlap each
-// other's load / MMA / store phases.
+// The kernel is a persistent, warp-specialized pipeline (one CTA per SM): a TMA producer
+// fills a 4- or 5-deep ring of FP32 tiles (two 128x32 boxes each, 128-byte swizzle = exactly the
+// UMMA K-major SW128 layout), four split warps turn ring tiles into operand tiles, one thread
+// issues the MMAs into one of two TMEM accumulators, and four epilogue warps read the
+// accumulator with tcgen05.ld (warp w owns TMEM lanes 32(w%4)..+31 = tile rows), write the
+// result swizzled back into the ring tile and TMA-store it.  Loads, splits, MMAs and stores of
+// consecutive tiles overlap.
 //
-// Every mbarrier wait is bounded: on expiry the CTA records an error code in *err, stops
-// issuing work, waits (bounded) for its own bulk stores, frees its TMEM and returns.
+// Every mbarrier wait is bounded: on expiry the role stops, the CTA records a nonzero code in
+// *err, and all roles leave their loops (the others' waits expire too); TMEM is freed after
+// the issuer has seen its last MMAs complete.
 #pragma once
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -32,39 +34,49 @@ namespace tc {
 
 constexpr int kRows = 128;          // arrays per tile (MMA M)
 constexpr int kCols = 64;           // elements per array (MMA N and K)
-constexpr int kThreads = 128;
 constexpr int kTmemCols = 64;
 constexpr uint32_t kSpinLimit = 1u << 26;   // bounded mbarrier polls (~seconds)
 
 enum Form { BF16X3 = 1, TF32X3 = 2 };
 
-// Shared-memory byte sizes of the operand images.
+// Shared-memory plan of the warp-specialized pipeline (per CTA, one CTA per SM):
+//   kStages FP32 tiles (TMA ring; a tile later holds the TF32 Xh split and finally the
+//   output tile for the TMA store), kABufs A-operand buffers (BF16: Xh|Xm|Xl, TF32: Xl),
+//   the B image, and the mbarriers.
+constexpr int kABufs = 2;
+constexpr int kAccs = 2;            // TMEM accumulators (64 columns each)
+constexpr int kTile = kRows * kCols * 4;   // FP32 tile bytes (32 KB)
+constexpr int kMaxStages = 5;
+
+// Splits live in the ring tile itself where they fit: a thread owns one tile row, reads its
+// 64 FP32 values into registers and overwrites the same bytes (BF16: Xh over the first
+// 128-byte box row, Xm over the second; TF32: Xh in place); only Xl needs an A buffer.
 template <int FORM> struct Sizes;
 template <> struct Sizes<BF16X3> {
-  static constexpr int kStage = kRows * kCols * 4;        // FP32 staging tile (TMA target)
-  static constexpr int kATile = kRows * kCols * 2;        // one bf16 A split (16 KB)
-  static constexpr int kANum = 3;
-  static constexpr int kBTile = kCols * kCols * 2;        // one bf16 B split (8 KB)
-  static constexpr int kBNum = 3;
+  static constexpr int kStages = 5;
+  static constexpr int kABuf = kRows * kCols * 2;         // Xl, bf16 (16 KB)
+  static constexpr int kBImage = 3 * kCols * kCols * 2;   // Kh|Km|Kl (24 KB)
 };
 template <> struct Sizes<TF32X3> {
-  static constexpr int kStage = kRows * kCols * 4;        // FP32 tile; becomes Xh in place
-  static constexpr int kATile = kRows * kCols * 4;        // Xl (32 KB)
-  static constexpr int kANum = 1;
-  static constexpr int kBTile = kCols * kCols * 4;        // one tf32 B split (16 KB)
-  static constexpr int kBNum = 2;
+  static constexpr int kStages = 4;
+  static constexpr int kABuf = kRows * kCols * 4;         // Xl, tf32 (32 KB)
+  static constexpr int kBImage = 2 * kCols * kCols * 4;   // Kh|Kl (32 KB)
 };
 
 template <int FORM>
 struct Layout {
   using S = Sizes<FORM>;
+  static constexpr int kStages = S::kStages;
   static constexpr int kStageOff = 0;
-  static constexpr int kAOff = kStageOff + S::kStage;
-  static constexpr int kBOff = kAOff + S::kANum * S::kATile;
-  static constexpr int kBarOff = kBOff + S::kBNum * S::kBTile;   // 2 mbarriers + tmem slot
-  static constexpr int kBytes = kBarOff + 64;
-  static constexpr int kDynamic = kBytes + 1024;                  // room for 1024-B alignment
-  static constexpr int kBImage = S::kBNum * S::kBTile;
+  static constexpr int kAOff = kStages * kTile;
+  static constexpr int kBOff = kAOff + kABufs * S::kABuf;
+  static constexpr int kBarOff = kBOff + S::kBImage;
+  // barriers: stage_full[5] stage_free[5] a_full[2] a_free[2] acc_full[2] acc_free[2], tmem slot
+  static constexpr int kTmemSlot = 8 * (2 * kMaxStages + 2 * kABufs + 2 * kAccs);
+  static constexpr int kBytes = kBarOff + kTmemSlot + 16;
+  static constexpr int kDynamic = kBytes + 1024;          // room for 1024-byte alignment
+  static constexpr int kBImage = S::kBImage;
+  static_assert(kDynamic <= 232448, "shared memory budget");
 };
 
 // Byte offset of 16-byte chunk `chunk` of row `row` in a K-major SW128 atom column
@@ -193,43 +205,50 @@ __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) 
   return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
 }
 
-// Splits the FP32 staging tile into the A operand tiles.  Thread t owns tile row t.
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void named_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Splits FP32 ring tile `stage` into A buffer `abuf` (thread r of 128 owns tile row r).
 template <int FORM>
-__device__ __forceinline__ void split_tile(uint8_t* base) {
-  using L = Layout<FORM>;
-  const uint32_t r = threadIdx.x;
-  uint8_t* stage = base + L::kStageOff;
-  uint8_t* a = base + L::kAOff;
+__device__ __forceinline__ void split_tile(uint8_t* stage, uint8_t* abuf, uint32_t r) {
   if constexpr (FORM == TF32X3) {
-    // elementwise: Xh = rna_tf32(X) in place, Xl = X - Xh in the second tile (same layout)
+    // elementwise: Xh = rna_tf32(X) in place, Xl = X - Xh into the A buffer (same layout)
 #pragma unroll
     for (int box = 0; box < 2; ++box)
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const uint32_t off = box * 16384u + sw128(r, j);
-        float4 v = *reinterpret_cast<const float4*>(stage + off);
+        const float4 v = *reinterpret_cast<const float4*>(stage + off);
         const uint32_t h0 = tf32_rna(v.x), h1 = tf32_rna(v.y), h2 = tf32_rna(v.z), h3 = tf32_rna(v.w);
-        float4 lo = make_float4(v.x - __uint_as_float(h0), v.y - __uint_as_float(h1),
-                                v.z - __uint_as_float(h2), v.w - __uint_as_float(h3));
+        const float4 lo = make_float4(v.x - __uint_as_float(h0), v.y - __uint_as_float(h1),
+                                      v.z - __uint_as_float(h2), v.w - __uint_as_float(h3));
         *reinterpret_cast<uint4*>(stage + off) = make_uint4(h0, h1, h2, h3);
-        *reinterpret_cast<float4*>(a + off) = lo;
+        *reinterpret_cast<float4*>(abuf + off) = lo;
       }
   } else {
-    // bf16 chunk j' holds elements 8j'..8j'+7 = fp32 chunks 2j', 2j'+1 of box j'/4
+    // Row r's 64 FP32 values (box 0 row r: elements 0..31, box 1 row r: 32..63) are read
+    // first; bf16 chunk j' (elements 8j'..8j'+7) of Xh then goes to box 0 row r, of Xm to box 1
+    // row r, of Xl to the A buffer, all in the K-major SW128 layout.
+    float x[64];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const float4 u = *reinterpret_cast<const float4*>(stage + (c >> 3) * 16384u + sw128(r, c & 7));
+      x[4 * c] = u.x; x[4 * c + 1] = u.y; x[4 * c + 2] = u.z; x[4 * c + 3] = u.w;
+    }
 #pragma unroll
     for (int jp = 0; jp < 8; ++jp) {
-      const int box = jp >> 2;
-      const int c0 = (2 * jp) & 7;
-      const float4 u = *reinterpret_cast<const float4*>(stage + box * 16384u + sw128(r, c0));
-      const float4 w = *reinterpret_cast<const float4*>(stage + box * 16384u + sw128(r, c0 + 1));
-      const float x[8] = {u.x, u.y, u.z, u.w, w.x, w.y, w.z, w.w};
       uint32_t hi[4], mid[4], lo[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         __nv_bfloat16 h[2], m[2], l[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-          const float v = x[2 * e + q];
+          const float v = x[8 * jp + 2 * e + q];
           h[q] = __float2bfloat16_rn(v);
           const float r1 = v - __bfloat162float(h[q]);
           m[q] = __float2bfloat16_rn(r1);
@@ -240,20 +259,21 @@ __device__ __forceinline__ void split_tile(uint8_t* base) {
         lo[e] = pack_bf16(l[0], l[1]);
       }
       const uint32_t off = sw128(r, jp);
-      *reinterpret_cast<uint4*>(a + 0 * 16384u + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-      *reinterpret_cast<uint4*>(a + 1 * 16384u + off) = make_uint4(mid[0], mid[1], mid[2], mid[3]);
-      *reinterpret_cast<uint4*>(a + 2 * 16384u + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+      *reinterpret_cast<uint4*>(stage + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+      *reinterpret_cast<uint4*>(stage + 16384u + off) = make_uint4(mid[0], mid[1], mid[2], mid[3]);
+      *reinterpret_cast<uint4*>(abuf + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
     }
   }
 }
 
-// Issues the split-product MMAs of one tile (one thread).
+// Issues the split-product MMAs of one tile (one thread).  sstage / sabuf / sb: shared
+// addresses of the ring tile, the A buffer and the B image.
 template <int FORM>
-__device__ __forceinline__ void issue_mmas(uint8_t* base, uint32_t tmem_d) {
-  using L = Layout<FORM>;
-  const uint32_t sbase = smem_u32(base);
+__device__ __forceinline__ void issue_mmas(uint32_t sstage, uint32_t sabuf, uint32_t sb, uint32_t tmem_d) {
   if constexpr (FORM == BF16X3) {
-    // (A split, B split) products, smallest magnitude first: A = {Xh, Xm, Xl}, B = {Kh, Km, Kl}
+    // (A split, B split) products, smallest magnitude first: A = {Xh, Xm, Xl}, B = {Kh, Km, Kl};
+    // Xh and Xm sit in the ring tile's two boxes, Xl in the A buffer.
+    const uint32_t asplit[3] = {sstage, sstage + 16384u, sabuf};
     constexpr int pa[6] = {2, 1, 0, 1, 0, 0};
     constexpr int pb[6] = {0, 1, 2, 0, 1, 0};
     constexpr uint32_t idesc = instr_desc(1);
@@ -261,13 +281,13 @@ __device__ __forceinline__ void issue_mmas(uint8_t* base, uint32_t tmem_d) {
     for (int p = 0; p < 6; ++p)
 #pragma unroll
       for (int k = 0; k < 4; ++k) {   // K = 16 bf16 = 32 bytes per MMA
-        const uint64_t ad = sw128_desc(sbase + L::kAOff + pa[p] * 16384u + k * 32u);
-        const uint64_t bd = sw128_desc(sbase + L::kBOff + pb[p] * 8192u + k * 32u);
+        const uint64_t ad = sw128_desc(asplit[pa[p]] + k * 32u);
+        const uint64_t bd = sw128_desc(sb + pb[p] * 8192u + k * 32u);
         umma(tmem_d, ad, bd, idesc, (p | k) ? 1u : 0u, BF16X3);
       }
   } else {
-    // A = {Xh (in the staging tile), Xl}, B = {Kh, Kl}; products Xl Kh, Xh Kl, Xh Kh
-    constexpr uint32_t aoff[3] = {(uint32_t)L::kAOff, (uint32_t)L::kStageOff, (uint32_t)L::kStageOff};
+    // A = {Xl (A buffer), Xh (ring tile), Xh}, B = {Kh, Kl, Kh}: products Xl Kh, Xh Kl, Xh Kh
+    const uint32_t abase[3] = {sabuf, sstage, sstage};
     constexpr int pb[3] = {0, 1, 0};
     constexpr uint32_t idesc = instr_desc(2);
 #pragma unroll
@@ -276,111 +296,187 @@ __device__ __forceinline__ void issue_mmas(uint8_t* base, uint32_t tmem_d) {
       for (int k = 0; k < 8; ++k) {   // K = 8 tf32 = 32 bytes per MMA; 32-element atoms
         const uint32_t koff = (k >> 2) * 16384u + (k & 3) * 32u;
         const uint32_t kboff = (k >> 2) * 8192u + (k & 3) * 32u;
-        const uint64_t ad = sw128_desc(sbase + aoff[p] + koff);
-        const uint64_t bd = sw128_desc(sbase + L::kBOff + pb[p] * 16384u + kboff);
+        const uint64_t ad = sw128_desc(abase[p] + koff);
+        const uint64_t bd = sw128_desc(sb + pb[p] * 16384u + kboff);
         umma(tmem_d, ad, bd, idesc, (p | k) ? 1u : 0u, TF32X3);
       }
   }
 }
 
+// Warp roles of k_tc8 (12 warps):
+//   warp 0 lane 0  TMA producer: ring tile s <- X tile j      (waits stage_free, arms stage_full)
+//                  (ring depth: 5 tiles for BF16x3, 4 for TF32x3)
+//   warp 1 lane 0  MMA issuer: TMEM acc t <- A buffer a . B    (waits a_full, acc_free;
+//                  commits to acc_full and a_free)
+//   warp 2         TMEM allocator / deallocator
+//   warps 4-7      split: ring tile s -> A buffer a            (waits stage_full, a_free)
+//   warps 8-11     epilogue: acc t -> registers -> ring tile s -> TMA store
+//                  (waits acc_full; frees acc t, then ring tile s once the store has read it)
+// Tile j of this CTA uses ring tile j % kStages, A buffer j % 2 and accumulator j % 2.
+constexpr int kWsThreads = 384;
+
+struct Bars {
+  uint32_t stage_full, stage_free, a_full, a_free, acc_full, acc_free;
+  __device__ Bars(uint32_t b)
+      : stage_full(b), stage_free(b + 8 * kMaxStages), a_full(b + 16 * kMaxStages),
+        a_free(b + 16 * kMaxStages + 8 * kABufs), acc_full(b + 16 * kMaxStages + 16 * kABufs),
+        acc_free(b + 16 * kMaxStages + 16 * kABufs + 8 * kAccs) {}
+};
+
 // x, y: tensor maps of the (batch x 64) FP32 matrices (box 32 x 128, SWIZZLE_128B).
 // bimage: the B operand shared-memory image (Layout<FORM>::kBImage bytes, 16-byte aligned).
 template <int FORM>
-__global__ void __launch_bounds__(kThreads) k_tc8(const __grid_constant__ CUtensorMap xmap,
-                                                  const __grid_constant__ CUtensorMap ymap,
-                                                  const uint4* __restrict__ bimage, int ntiles,
-                                                  int* __restrict__ err) {
+__global__ void __launch_bounds__(kWsThreads, 1) k_tc8(const __grid_constant__ CUtensorMap xmap,
+                                                        const __grid_constant__ CUtensorMap ymap,
+                                                        const uint4* __restrict__ bimage, int ntiles,
+                                                        int* __restrict__ err) {
   using L = Layout<FORM>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const uint32_t bar_load = smem_u32(base + L::kBarOff);
-  const uint32_t bar_mma = bar_load + 8;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + L::kBarOff + 16);
-  __shared__ int s_abort;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t sbase = smem_u32(base);
+  const Bars bars(sbase + L::kBarOff);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + L::kBarOff + L::kTmemSlot);
+  constexpr int kStages = L::kStages;
+  __shared__ volatile int s_abort;
+  __shared__ volatile int s_group_ok[2];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntile_local = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
   if (tid == 0) {
     s_abort = 0;
-    mbar_init(bar_load, 1);
-    mbar_init(bar_mma, 1);
+    for (int i = 0; i < kStages; ++i) {
+      mbar_init(bars.stage_full + 8 * i, 1);
+      mbar_init(bars.stage_free + 8 * i, 1);
+    }
+    for (int i = 0; i < kABufs; ++i) {
+      mbar_init(bars.a_full + 8 * i, 1);
+      mbar_init(bars.a_free + 8 * i, 1);
+    }
+    for (int i = 0; i < kAccs; ++i) {
+      mbar_init(bars.acc_full + 8 * i, 1);
+      mbar_init(bars.acc_free + 8 * i, 1);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == 2) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(kTmemCols));
+                 "r"(kAccs * kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  // B operand image: plain copy, once per CTA
   {
     uint4* dst = reinterpret_cast<uint4*>(base + L::kBOff);
-    for (int i = tid; i < L::kBImage / 16; i += kThreads) dst[i] = __ldg(bimage + i);
+    for (int i = tid; i < L::kBImage / 16; i += kWsThreads) dst[i] = __ldg(bimage + i);
   }
   fence_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem_d = *tmem_slot;
-  uint32_t phase = 0;
+  const uint32_t tmem_base = *tmem_slot;
   bool ok = true;
 
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    if (tid == 0) {
-      bulk_wait_read0();                                // previous tile's store has read its staging
-      mbar_expect_tx(bar_load, 2u * 16384u);
-      tma_load_2d(smem_u32(base + L::kStageOff), &xmap, 0, tile * kRows, bar_load);
-      tma_load_2d(smem_u32(base + L::kStageOff) + 16384u, &xmap, 32, tile * kRows, bar_load);
+  if (warp == 0 && lane == 0) {
+    for (int j = 0; j < ntile_local && ok && !s_abort; ++j) {
+      const int s = j % kStages;
+      const uint32_t ph = (uint32_t)(j / kStages) & 1u;
+      ok = mbar_wait(bars.stage_free + 8 * s, ph ^ 1u);
+      if (!ok) break;
+      const int tile = blockIdx.x + j * gridDim.x;
+      const uint32_t dst = sbase + L::kStageOff + s * kTile;
+      mbar_expect_tx(bars.stage_full + 8 * s, kTile);
+      tma_load_2d(dst, &xmap, 0, tile * kRows, bars.stage_full + 8 * s);
+      tma_load_2d(dst + 16384u, &xmap, 32, tile * kRows, bars.stage_full + 8 * s);
     }
-    ok = mbar_wait(bar_load, phase);
-    if (__syncthreads_or(!ok)) break;
-    split_tile<FORM>(base);
-    fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (tid == 0) {
-      issue_mmas<FORM>(base, tmem_d);
-      umma_commit(bar_mma);
+  } else if (warp == 1 && lane == 0) {
+    for (int j = 0; j < ntile_local && ok && !s_abort; ++j) {
+      const int s = j % kStages, a = j % kABufs, t = j % kAccs;
+      ok = mbar_wait(bars.a_full + 8 * a, (uint32_t)(j / kABufs) & 1u);
+      if (ok) ok = mbar_wait(bars.acc_free + 8 * t, ((uint32_t)(j / kAccs) & 1u) ^ 1u);
+      if (!ok) break;
+      tc_fence_after();
+      issue_mmas<FORM>(sbase + L::kStageOff + s * kTile, sbase + L::kAOff + a * Sizes<FORM>::kABuf,
+                       sbase + L::kBOff, tmem_base + t * kTmemCols);
+      umma_commit(bars.acc_full + 8 * t);
+      umma_commit(bars.a_free + 8 * a);
     }
-    ok = mbar_wait(bar_mma, phase);
-    if (__syncthreads_or(!ok)) break;
-    tc_fence_after();
-    // epilogue: TMEM lane (32 warp + lane) = tile row; 64 FP32 columns -> swizzled staging
-    {
-      const uint32_t row = tid;
-      const uint32_t lane_addr = tmem_d + ((uint32_t)(warp * 32) << 16);
+    if (ok && ntile_local > 0) {   // the last MMAs must finish before TMEM is freed
+      const int j = ntile_local - 1;
+      ok = mbar_wait(bars.a_free + 8 * (j % kABufs), (uint32_t)(j / kABufs) & 1u);
+    }
+  } else if (warp >= 4 && warp < 8) {
+    // Only the group leader polls the mbarriers (bounded) and broadcasts the outcome, so the
+    // group's named barrier is reached by all 128 threads whatever the outcome.
+    const uint32_t r = tid - 128;
+    for (int j = 0; j < ntile_local; ++j) {
+      const int s = j % kStages, a = j % kABufs;
+      if (r == 0) {
+        bool g = !s_abort && mbar_wait(bars.stage_full + 8 * s, (uint32_t)(j / kStages) & 1u);
+        if (g) g = mbar_wait(bars.a_free + 8 * a, ((uint32_t)(j / kABufs) & 1u) ^ 1u);
+        s_group_ok[0] = g ? 1 : 0;
+      }
+      named_sync(1, 128);
+      if (!s_group_ok[0]) {
+        ok = r != 0;      // the leader reports the expiry
+        break;
+      }
+      split_tile<FORM>(base + L::kStageOff + s * kTile, base + L::kAOff + a * Sizes<FORM>::kABuf, r);
+      fence_async_smem();
+      named_sync(1, 128);
+      if (r == 0) mbar_arrive(bars.a_full + 8 * a);
+    }
+  } else if (warp >= 8) {
+    const uint32_t r = tid - 256;               // tile row = TMEM lane
+    const uint32_t quarter = (uint32_t)(warp & 3) * 32u;
+    for (int j = 0; j < ntile_local; ++j) {
+      const int s = j % kStages, t = j % kAccs;
+      if (r == 0) s_group_ok[1] = (!s_abort && mbar_wait(bars.acc_full + 8 * t, (uint32_t)(j / kAccs) & 1u)) ? 1 : 0;
+      named_sync(2, 128);
+      if (!s_group_ok[1]) {
+        ok = r != 0;
+        break;
+      }
+      tc_fence_after();
+      float v[64];
+      const uint32_t taddr = tmem_base + t * kTmemCols + (quarter << 16);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        float v[16];
-        tmem_ld16(lane_addr + q * 16, v);
-        tmem_wait_ld();
+        float w[16];
+        tmem_ld16(taddr + q * 16, w);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int col = q * 16 + c * 4;
-          const uint32_t off = (col >> 5) * 16384u + sw128(row, (col & 31) >> 2);
-          *reinterpret_cast<float4*>(base + L::kStageOff + off) =
-              make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
-        }
+        for (int i = 0; i < 16; ++i) v[q * 16 + i] = w[i];
+      }
+      tmem_wait_ld();
+      tc_fence_before();
+      named_sync(2, 128);
+      if (r == 0) mbar_arrive(bars.acc_free + 8 * t);
+      uint8_t* out = base + L::kStageOff + s * kTile;
+#pragma unroll
+      for (int c = 0; c < 16; ++c) {
+        const int col = c * 4;
+        const uint32_t off = (col >> 5) * 16384u + sw128(r, (col & 31) >> 2);
+        *reinterpret_cast<float4*>(out + off) = make_float4(v[col], v[col + 1], v[col + 2], v[col + 3]);
+      }
+      fence_async_smem();
+      named_sync(2, 128);
+      if (r == 0) {
+        const int tile = blockIdx.x + j * gridDim.x;
+        tma_store_2d(&ymap, 0, tile * kRows, sbase + L::kStageOff + s * kTile);
+        tma_store_2d(&ymap, 32, tile * kRows, sbase + L::kStageOff + s * kTile + 16384u);
+        bulk_commit();
+        bulk_wait_read0();
+        mbar_arrive(bars.stage_free + 8 * s);
       }
     }
-    fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-    if (tid == 0) {
-      tma_store_2d(&ymap, 0, tile * kRows, smem_u32(base + L::kStageOff));
-      tma_store_2d(&ymap, 32, tile * kRows, smem_u32(base + L::kStageOff) + 16384u);
-      bulk_commit();
-    }
-    phase ^= 1u;
+    if (r == 0) bulk_wait0();
   }
-  if (tid == 0) {
-    bulk_wait0();
-    if (!ok) atomicExch(err, 1);
+  if (!ok) {
+    s_abort = 1;
+    atomicExch(err, 1);
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(kTmemCols));
+  if (warp == 2) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kAccs * kTmemCols));
   }
 }
 

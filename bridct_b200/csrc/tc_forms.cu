@@ -158,7 +158,7 @@ int launch_tc8(const bridct_plan* p, int inverse, const float* x, float* y, size
   static const int bps = [&]() {
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kDynamic) != cudaSuccess) return 0;
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, tc::kThreads, L::kDynamic) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, tc::kWsThreads, L::kDynamic) != cudaSuccess) return 0;
     return b;
   }();
   if (bps <= 0) return cuda_fail(cudaErrorInvalidConfiguration, "k_tc8 occupancy");
@@ -170,7 +170,7 @@ int launch_tc8(const bridct_plan* p, int inverse, const float* x, float* y, size
   const int ntiles = (int)((batch + tc::kRows - 1) / tc::kRows);
   int grid = p->dev->sm_count * bps;
   if (grid > ntiles) grid = ntiles;
-  k<<<grid, tc::kThreads, L::kDynamic, st>>>(xm, ym, reinterpret_cast<const uint4*>(d->images[FORM][inverse]),
+  k<<<grid, tc::kWsThreads, L::kDynamic, st>>>(xm, ym, reinterpret_cast<const uint4*>(d->images[FORM][inverse]),
                                                ntiles, d->err);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_tc8 launch");
