@@ -271,6 +271,7 @@ def main():
     import torch.distributed as dist
 
     from bridct_b200 import _lib, torch_api
+    from bridct_b200.dist import max_over_ranks
     from oracle import oracle as O
 
     torch.cuda.set_device(local)
@@ -339,10 +340,7 @@ def main():
         if world > 1:
             dist.barrier()
         ms = start.elapsed_time(end)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dev)
         timings[name] = {"ms_total": ms, "ms_per_step": ms / args.steps, "clocks": clk.summary(),
                          "gbs": bytes_step * args.steps * world / (ms * 1e-3) / 1e9}
         del graphs
@@ -370,10 +368,7 @@ def main():
     for _ in range(e2e_steps):
         _lib.check(lib.bridct_plan_apply_batch(plan, mode, hin.data_ptr(), hout.data_ptr(), b))
     e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dev)
     e2e = {"value": bytes_step * e2e_steps * world / e2e_s / 1e9, "unit": "GB/s",
            "h2d_bytes_per_step": int(4 * b * h * w), "d2h_bytes_per_step": int(4 * b * h * w),
            "form": "sj", "ms_per_step": 1e3 * e2e_s / e2e_steps}
