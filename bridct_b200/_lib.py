@@ -23,6 +23,11 @@ class RaggedItem(C.Structure):
                 ("offset", C.c_size_t)]
 
 
+class RaggedTuning(C.Structure):
+    _fields_ = [("tile_floats", C.c_int), ("strip_floats", C.c_int), ("row_floats", C.c_int),
+                ("lookahead", C.c_int)]
+
+
 def _sig(lib, name, restype, argtypes):
     f = getattr(lib, name)
     f.restype = restype
@@ -61,11 +66,14 @@ def lib() -> C.CDLL:
 
 # Entry points added by later translation units (bound when present).
 EXTRA_SIGNATURES = [
+    ("bridct_ragged_default_tuning", None, [C.POINTER(RaggedTuning)]),
     ("bridct_ragged_create", C.c_void_p, [C.POINTER(RaggedItem), C.c_size_t]),
+    ("bridct_ragged_create_tuned", C.c_void_p, [C.POINTER(RaggedItem), C.c_size_t, C.POINTER(RaggedTuning)]),
     ("bridct_ragged_destroy", None, [C.c_void_p]),
+    ("bridct_ragged_units", C.c_size_t, [C.c_void_p]),
     ("bridct_ragged_apply_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("bridct_ragged_apply_loop_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
-    ("bridct_ragged_route", C.c_char_p, [C.c_void_p]),
+    ("bridct_ragged_timeout_flag", C.c_int, [C.c_void_p]),
     ("bridct_device_timeout_flag", C.c_int, [C.c_int]),
 ]
 

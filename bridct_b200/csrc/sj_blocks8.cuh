@@ -24,17 +24,7 @@ __device__ __forceinline__ int b8_slot(int chunk) {
 
 template <int MODE>
 __device__ __forceinline__ void b8_transform(float (&v)[64]) {
-  // rows (contiguous 8-float lines)
-#pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    float t[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) t[c] = v[r * 8 + c];
-    reg_line_apply<8, MODE>(t);
-#pragma unroll
-    for (int c = 0; c < 8; ++c) v[r * 8 + c] = t[c];
-  }
-  // columns
+  // columns, then rows (the reference's vertical-then-bands order, src/generated/rect.c:5-15)
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
     float t[8];
@@ -43,6 +33,15 @@ __device__ __forceinline__ void b8_transform(float (&v)[64]) {
     reg_line_apply<8, MODE>(t);
 #pragma unroll
     for (int r = 0; r < 8; ++r) v[r * 8 + c] = t[r];
+  }
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    float t[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) t[c] = v[r * 8 + c];
+    reg_line_apply<8, MODE>(t);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) v[r * 8 + c] = t[c];
   }
 }
 

@@ -53,6 +53,43 @@ BRIDCT_API int bridct_plan_apply_form_device(bridct_plan *plan, enum bridct_mode
  * mbarrier wait expired (the kernel then skipped its remaining tiles and returned). */
 BRIDCT_API int bridct_device_timeout_flag(int device);
 
+/* ---- Batching form: mixed shapes and directions in one persistent launch ---------------- */
+
+/* One array of a ragged batch: shape, mode (enum bridct_mode) and offset, in floats, from the
+ * batch base pointers (a multiple of 4, so every array is 16-byte aligned). */
+typedef struct {
+    int height, width, mode, reserved;
+    size_t offset;
+} bridct_ragged_item;
+
+/* Work-unit geometry of a ragged batch (chosen per shape class by the autotuner). */
+typedef struct {
+    int tile_floats;   /* arrays up to this many floats run both passes in one unit (<= 16384) */
+    int strip_floats;  /* floats per column-strip unit of a larger array (<= 16384)            */
+    int row_floats;    /* floats per row-block unit of a larger array (<= 16384)               */
+    int lookahead;     /* larger arrays whose strips are queued ahead of a row pass (1..64)   */
+} bridct_ragged_tuning;
+
+typedef struct bridct_ragged bridct_ragged;
+
+BRIDCT_API void bridct_ragged_default_tuning(bridct_ragged_tuning *tuning);
+/* Validates the items (supported shapes and modes, aligned, non-overlapping) and builds the
+ * device work queue; NULL on error (see bridct_last_error). */
+BRIDCT_API bridct_ragged *bridct_ragged_create(const bridct_ragged_item *items, size_t count);
+BRIDCT_API bridct_ragged *bridct_ragged_create_tuned(const bridct_ragged_item *items, size_t count,
+                                                     const bridct_ragged_tuning *tuning);
+BRIDCT_API void bridct_ragged_destroy(bridct_ragged *batch);
+BRIDCT_API size_t bridct_ragged_units(const bridct_ragged *batch);
+/* One persistent launch over the whole batch (device pointers, asynchronous on `stream`,
+ * capturable in a CUDA graph: a counter reset and one kernel). */
+BRIDCT_API int bridct_ragged_apply_device(bridct_ragged *batch, const float *input, float *output,
+                                          void *stream);
+/* The same batch as one plain-form launch per array (the comparison baseline). */
+BRIDCT_API int bridct_ragged_apply_loop_device(bridct_ragged *batch, const float *input,
+                                               float *output, void *stream);
+/* Reads and clears the batch's bounded-wait flag (nonzero: a dependency wait expired). */
+BRIDCT_API int bridct_ragged_timeout_flag(bridct_ragged *batch);
+
 /* Waits for all work queued on the plan's own stream. */
 BRIDCT_API int bridct_plan_synchronize(bridct_plan *plan);
 

@@ -1,0 +1,97 @@
+"""Batching form: one persistent launch over mixed shapes and directions, against float64 per
+array, the per-array launch loop and other unit geometries (all within the parity bound)."""
+import numpy as np
+import pytest
+import torch
+
+from bridct_b200.ragged import RaggedBatch
+from oracle import oracle as O
+from tests.helpers import SIZES, TOL
+
+pytestmark = pytest.mark.gpu
+
+
+def random_batch(n, seed, max_elems=1 << 20):
+    rng = np.random.default_rng(seed)
+    items = []
+    while len(items) < n:
+        h, w = int(rng.choice(SIZES)), int(rng.choice(SIZES))
+        if h * w <= max_elems:
+            items.append((h, w, int(rng.integers(0, 3))))
+    return items
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_ragged_all_shapes_vs_fp64(seed):
+    items = random_batch(160, seed)
+    items += [(h, w, m) for h in SIZES for w in SIZES for m in (0, 1) if (h * w) <= 65536][: 40]
+    b = RaggedBatch(items)
+    rng = np.random.default_rng(seed + 10)
+    x = torch.from_numpy(rng.uniform(-1, 1, b.span).astype(np.float32)).cuda()
+    y = b.apply(x)
+    torch.cuda.synchronize()
+    assert not b.timed_out()
+    ys = [t.cpu().numpy() for t in b.unpack(y)]
+    xs = [t.cpu().numpy() for t in b.unpack(x)]
+    for (h, w, m), xi, yi in zip(items, xs, ys):
+        assert O.rel_max_error(yi, O.fp64_apply(xi, m), xi, output_scaled=True) <= TOL, (h, w, m)
+
+
+def close(a, b, x, items, batch):
+    for (h, w, m), xa, ya, yb in zip(items, batch.unpack(x), batch.unpack(a), batch.unpack(b)):
+        xa, ya, yb = xa.cpu().numpy(), ya.cpu().numpy(), yb.cpu().numpy()
+        assert O.rel_max_error(ya, yb, xa, output_scaled=True) <= TOL, (h, w, m)
+
+
+def test_ragged_matches_launch_loop():
+    items = random_batch(120, 5)
+    b = RaggedBatch(items)
+    x = torch.randn(b.span, device="cuda")
+    y1 = b.apply(x)
+    y2 = b.apply_loop(x)
+    torch.cuda.synchronize()
+    assert not b.timed_out()
+    close(y1, y2, x, items, b)
+
+
+@pytest.mark.parametrize("tuning", [dict(tile_floats=4096, strip_floats=4096, row_floats=4096, lookahead=1),
+                                    dict(tile_floats=16384, strip_floats=8192, row_floats=16384, lookahead=8)])
+def test_ragged_tunings_agree(tuning):
+    items = random_batch(60, 9)
+    x = torch.randn(RaggedBatch(items).span, device="cuda")
+    b = RaggedBatch(items)
+    ref = b.apply(x)
+    got = RaggedBatch(items, tuning=tuning).apply(x)
+    torch.cuda.synchronize()
+    close(ref, got, x, items, b)
+
+
+def test_ragged_graph_capture_and_replay():
+    items = random_batch(64, 3)
+    b = RaggedBatch(items)
+    x = torch.randn(b.span, device="cuda")
+    y = torch.empty_like(x)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        b.apply(x, y)
+    s.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        b.apply(x, y, stream=s.cuda_stream)
+    y.zero_()
+    with torch.cuda.stream(s):
+        g.replay()
+        g.replay()
+    s.synchronize()
+    ref = b.apply(x)
+    torch.cuda.synchronize()
+    assert torch.equal(y, ref)          # the same kernel, replayed from the graph
+
+
+def test_ragged_rejects_bad_items():
+    with pytest.raises(ValueError):
+        RaggedBatch([(8, 12, 0)])
+    with pytest.raises(ValueError):
+        RaggedBatch([(8, 8, 0), (8, 8, 0)], offsets=[0, 32])     # overlap
+    with pytest.raises(ValueError):
+        RaggedBatch([(8, 8, 0)], offsets=[2])                    # misaligned
