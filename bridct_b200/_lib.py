@@ -75,6 +75,8 @@ EXTRA_SIGNATURES = [
     ("bridct_ragged_apply_loop_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("bridct_ragged_timeout_flag", C.c_int, [C.c_void_p]),
     ("bridct_device_timeout_flag", C.c_int, [C.c_int]),
+    ("bridct_ragged_apply_noalloc", C.c_int, [C.POINTER(RaggedItem), C.c_size_t, C.c_void_p, C.c_void_p,
+                                              C.c_void_p]),
 ]
 
 

@@ -56,11 +56,10 @@ double sj_scale(int n, int k) {
 }
 
 // Four-step tables for N = 32 G (see sj_lines.cuh): twiddles w_N^{bc} s(32,c) and the
-// post-rotation coefficients with s(G,d) and the orthonormal factor folded in.
-static void build_fourstep_tables(int N, std::vector<float2>& tw, std::vector<float4>& post) {
+// post-rotation coefficients with s(G,d) and the orthonormal factor folded in.  Fills
+// caller-provided arrays of G*17 float2 and 17*G float4.
+void fill_fourstep_tables(int N, float2* tw, float4* post) {
   const int G = N / 32;
-  tw.assign((size_t)G * 17, float2{0, 0});
-  post.assign((size_t)17 * G, float4{0, 0, 0, 0});
   for (int b = 0; b < G; ++b)
     for (int c = 0; c < 17; ++c) {
       const double ang = -2 * M_PI * (double)b * c / N;
@@ -79,6 +78,13 @@ static void build_fourstep_tables(int N, std::vector<float2>& tw, std::vector<fl
       p.w = k ? (float)(-sig(N - k) * sg * std::cos(th)) : 0.f;
       post[(size_t)c * G + d] = p;
     }
+}
+
+void build_fourstep_tables(int N, std::vector<float2>& tw, std::vector<float4>& post) {
+  const int G = N / 32;
+  tw.assign((size_t)G * 17, float2{0, 0});
+  post.assign((size_t)17 * G, float4{0, 0, 0, 0});
+  fill_fourstep_tables(N, tw.data(), post.data());
 }
 
 void plain_table_h8(PlainLauncher (*row)[3]);

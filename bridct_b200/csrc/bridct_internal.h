@@ -25,6 +25,9 @@ struct DeviceCtx {
 void set_error(const std::string& s);
 int cuda_fail(cudaError_t e, const char* what);
 double sj_scale(int n, int k);
+// Four-step tables of line length N (twiddles, post-rotation coefficients), float64-derived.
+void build_fourstep_tables(int N, std::vector<float2>& tw, std::vector<float4>& post);
+void fill_fourstep_tables(int N, float2* tw, float4* post);
 DeviceCtx* device_ctx(int device);
 int current_device(int* dev);
 const void* device_address(const void* p, bool* pinned);

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "../../include/bridct_b200.h"
@@ -277,3 +278,202 @@ BRIDCT_API int bridct_ragged_apply_loop_device(bridct_ragged* r, const float* x,
 }
 
 }  // extern "C"
+
+// ---- Ragged batch without any allocation ---------------------------------------------------
+//
+// Some callers cannot let a library allocate device memory: a framework whose caching
+// allocator owns every byte of the GPU (any cudaMalloc outside it can fail or fragment its
+// pool), a latency-bound loop where cudaMalloc/cudaFree's implicit device synchronisation is
+// not acceptable, or an embedding that fixes the process's device footprint at start-up.
+// bridct_ragged_apply_noalloc serves them: the caller passes the item list and the input and
+// output buffers, and everything else the persistent kernel needs (work queue, per-array
+// counters, error word, four-step tables) lives in one statically sized __device__ array below,
+// which every GPU that loads this library holds until the process exits.  The host side builds
+// the queue in static buffers as well, so a successful call allocates nothing.
+namespace {
+
+constexpr int kNaMaxArrays = 4096;    // items per call
+constexpr int kNaMaxUnits = 49152;    // work units per call (default unit geometry)
+constexpr int kNaTw = 17 * (4 + 8 + 16 + 32);     // float2 twiddles, N = 128..1024
+constexpr int kNaPost = 17 * (4 + 8 + 16 + 32);   // float4 post coefficients, N = 128..1024
+
+struct NaOff {
+  static constexpr size_t arrays = 0;
+  static constexpr size_t units = arrays + sizeof(bridct::RaggedArray) * kNaMaxArrays;
+  static constexpr size_t counters = units + sizeof(bridct::RaggedUnit) * kNaMaxUnits;
+  static constexpr size_t err = counters + sizeof(unsigned int) * (kNaMaxArrays + 1);
+  static constexpr size_t tw = (err + sizeof(int) + 255) / 256 * 256;
+  static constexpr size_t post = tw + sizeof(float2) * kNaTw;
+  static constexpr size_t bytes = post + sizeof(float4) * kNaPost;
+};
+static_assert(NaOff::post % 16 == 0, "post table alignment");
+
+}  // namespace
+
+// About 0.9 MB: queue (arrays, units), counters, error word, four-step tables.  Host code must
+// not use this name as a device address; the entry point resolves it per device below.
+static __device__ __align__(256) unsigned char g_ragged_scratch[NaOff::bytes];
+
+namespace {
+
+std::mutex g_na_mutex;                                  // one call at a time (shared scratch)
+bridct::RaggedArray g_na_arrays[kNaMaxArrays];
+bridct::RaggedUnit g_na_units[kNaMaxUnits];
+int g_na_big[kNaMaxArrays];
+int g_na_small[kNaMaxArrays];
+int g_na_order[kNaMaxArrays];
+float2 g_na_tw[kNaTw];
+float4 g_na_post[kNaPost];
+bool g_na_tables = false;
+unsigned char* g_na_addr[64] = {};                      // scratch address per device
+
+int na_segment(int i) { return 17 * ((4 << i) - 4); }  // first entry of N = 128 << i
+
+}  // namespace
+
+extern "C" BRIDCT_API int bridct_ragged_apply_noalloc(const bridct_ragged_item* items, size_t count,
+                                                      const float* input, float* output, void* stream) {
+  using namespace bridct;
+  if (!items || !input || !output || count == 0) return BRIDCT_INVALID_ARGUMENT;
+  if (count > (size_t)kNaMaxArrays) {
+    set_error("bridct_ragged_apply_noalloc: at most 4096 arrays per call");
+    return BRIDCT_INVALID_ARGUMENT;
+  }
+  std::lock_guard<std::mutex> lock(g_na_mutex);
+  // validation (as bridct_ragged_create): shapes, modes, 16-byte aligned offsets, no overlap
+  size_t span = 0;
+  for (size_t i = 0; i < count; ++i) {
+    const bridct_ragged_item& it = items[i];
+    if (!bridct_supported(it.height, it.width) || it.mode < 0 || it.mode > 2 || it.offset % 4) {
+      set_error("bridct_ragged_apply_noalloc: unsupported shape or mode, or misaligned offset");
+      return BRIDCT_INVALID_ARGUMENT;
+    }
+    span = std::max(span, it.offset + (size_t)it.height * it.width);
+    g_na_order[i] = (int)i;
+  }
+  std::sort(g_na_order, g_na_order + count, [&](int a, int b) {
+    return items[a].offset != items[b].offset ? items[a].offset < items[b].offset : a < b;
+  });
+  for (size_t i = 1; i < count; ++i) {
+    const bridct_ragged_item& p = items[g_na_order[i - 1]];
+    if (items[g_na_order[i]].offset < p.offset + (size_t)p.height * p.width) {
+      set_error("bridct_ragged_apply_noalloc: arrays overlap");
+      return BRIDCT_INVALID_ARGUMENT;
+    }
+  }
+  const uintptr_t xa = (uintptr_t)input, ya = (uintptr_t)output;
+  if ((xa <= ya ? ya - xa : xa - ya) < span * sizeof(float)) return BRIDCT_OVERLAPPING_BUFFERS;
+  if ((xa | ya) % 16) return BRIDCT_BAD_ALIGNMENT;
+
+  // work queue with the default unit geometry (same units as bridct_ragged_create)
+  bridct_ragged_tuning t;
+  bridct_ragged_default_tuning(&t);
+  int nbig = 0, nsmall = 0;
+  for (size_t i = 0; i < count; ++i) {
+    const bridct_ragged_item& it = items[i];
+    RaggedArray a{(long long)it.offset, it.height, it.width, it.mode, 0};
+    if ((long long)it.height * it.width <= t.tile_floats) {
+      g_na_small[nsmall++] = (int)i;
+    } else {
+      a.nstrips = it.width / strip_cols(it.height, it.width, t.strip_floats);
+      g_na_big[nbig++] = (int)i;
+    }
+    g_na_arrays[i] = a;
+  }
+  auto size_desc = [&](int a, int b) {
+    const long long ea = (long long)items[a].height * items[a].width;
+    const long long eb = (long long)items[b].height * items[b].width;
+    return ea != eb ? ea > eb : a < b;
+  };
+  std::sort(g_na_big, g_na_big + nbig, size_desc);
+  std::sort(g_na_small, g_na_small + nsmall, size_desc);
+  int nunits = 0;
+  bool full = false;
+  auto push = [&](RaggedUnit u) {
+    if (nunits == kNaMaxUnits) full = true;
+    else g_na_units[nunits++] = u;
+  };
+  for (int k = 0; k < nbig + t.lookahead; ++k) {
+    if (k < nbig) {
+      const RaggedArray& a = g_na_arrays[g_na_big[k]];
+      const int tc = a.w / a.nstrips;
+      for (int s = 0; s < a.nstrips; ++s) push(RaggedUnit{g_na_big[k], UNIT_COLSTRIP, s * tc, tc});
+    }
+    if (k >= t.lookahead) {
+      const int i = g_na_big[k - t.lookahead];
+      const RaggedArray& a = g_na_arrays[i];
+      const int rb = block_rows(a.h, a.w, t.row_floats);
+      for (int r0 = 0; r0 < a.h; r0 += rb) push(RaggedUnit{i, UNIT_ROWBLOCK, r0, rb});
+    }
+  }
+  for (int k = 0; k < nsmall; ++k) push(RaggedUnit{g_na_small[k], UNIT_TILE, 0, 0});
+  if (full) {
+    set_error("bridct_ragged_apply_noalloc: the batch needs more than 49152 work units");
+    return BRIDCT_INVALID_ARGUMENT;
+  }
+
+  // set-up, once per device, with that device current: resolve the scratch array's device
+  // address (the host-side name is only a stand-in) and upload the four-step tables into it
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return BRIDCT_INVALID_ARGUMENT;
+  if (!g_na_tables) {
+    for (int i = 0; i < 4; ++i) fill_fourstep_tables(128 << i, g_na_tw + na_segment(i), g_na_post + na_segment(i));
+    g_na_tables = true;
+  }
+  if (!g_na_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_ragged_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_ragged_scratch)");
+    unsigned char* base = static_cast<unsigned char*>(p);
+    e = cudaMemcpy(base + NaOff::tw, g_na_tw, sizeof(g_na_tw), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(base + NaOff::post, g_na_post, sizeof(g_na_post), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "scratch tables");
+    g_na_addr[dev] = base;
+  }
+  static int bps = [] {
+    if (cudaFuncSetAttribute(k_ragged, cudaFuncAttributeMaxDynamicSharedMemorySize, kRaggedSmem) != cudaSuccess)
+      return 0;
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_ragged, kRaggedThreads, kRaggedSmem) != cudaSuccess) return 0;
+    return b;
+  }();
+  int sms = 0;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess || bps <= 0) return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidConfiguration, "k_ragged");
+  unsigned char* base = g_na_addr[dev];
+  cudaStream_t st = (cudaStream_t)stream;
+  // The scratch keeps the previous call's contents: queue tables are overwritten, and the
+  // counters and error word are cleared before the launch.
+  e = cudaMemcpyAsync(base + NaOff::arrays, g_na_arrays, count * sizeof(RaggedArray), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + NaOff::units, g_na_units, (size_t)nunits * sizeof(RaggedUnit), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + NaOff::counters, 0, (count + 1) * sizeof(unsigned int), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + NaOff::err, 0, sizeof(int), st);
+  if (e != cudaSuccess) return cuda_fail(e, "scratch upload");
+  RaggedArgs args;
+  args.x = input;
+  args.y = output;
+  args.arrays = reinterpret_cast<const RaggedArray*>(base + NaOff::arrays);
+  args.units = reinterpret_cast<const RaggedUnit*>(base + NaOff::units);
+  args.nunits = nunits;
+  args.next = reinterpret_cast<unsigned int*>(base + NaOff::counters);
+  args.done = args.next + 1;
+  args.err = reinterpret_cast<int*>(base + NaOff::err);
+  for (int i = 0; i < 4; ++i) {
+    args.tab[i].tw = reinterpret_cast<const float2*>(base + NaOff::tw) + na_segment(i);
+    args.tab[i].post = reinterpret_cast<const float4*>(base + NaOff::post) + na_segment(i);
+  }
+  const int grid = (int)std::min<long long>((long long)sms * bps, nunits);
+  k_ragged<<<grid, kRaggedThreads, kRaggedSmem, st>>>(args);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "k_ragged launch");
+  // Synchronous: the shared scratch is free again when the call returns.
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "bridct_ragged_apply_noalloc");
+  int flag = 0;
+  e = cudaMemcpy(&flag, base + NaOff::err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "error word");
+  return flag ? BRIDCT_TIMEOUT : BRIDCT_OK;
+}

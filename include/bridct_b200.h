@@ -90,6 +90,21 @@ BRIDCT_API int bridct_ragged_apply_loop_device(bridct_ragged *batch, const float
 /* Reads and clears the batch's bounded-wait flag (nonzero: a dependency wait expired). */
 BRIDCT_API int bridct_ragged_timeout_flag(bridct_ragged *batch);
 
+/* No counterpart in the reference.  The ragged batch for callers that cannot let a library
+ * allocate device memory (a framework whose caching allocator owns the whole GPU, a loop that
+ * cannot afford cudaMalloc's implicit synchronisation, a fixed device footprint): the items and
+ * the input/output buffers are passed in, and the work queue, counters and tables live in one
+ * static device array of about 0.9 MB that every GPU loading this library holds until exit.
+ * Limits: at most 4096 arrays and 49152 work units per call (default unit geometry), else
+ * BRIDCT_INVALID_ARGUMENT with a message.  A successful call allocates nothing.  The first call
+ * on a device resolves that array's address and uploads the four-step tables into it, so make
+ * it before any stream capture.  Every call shares the array and overwrites the previous call's
+ * queue; calls are serialized and synchronous (they return after their kernel finished),
+ * because two calls overlapping on the GPU would race on it.  Returns BRIDCT_TIMEOUT if a
+ * bounded dependency wait expired. */
+BRIDCT_API int bridct_ragged_apply_noalloc(const bridct_ragged_item *items, size_t count,
+                                           const float *input, float *output, void *stream);
+
 /* Waits for all work queued on the plan's own stream. */
 BRIDCT_API int bridct_plan_synchronize(bridct_plan *plan);
 
