@@ -262,6 +262,7 @@ def main():
     ap.add_argument("--workload", default="blocks8")
     ap.add_argument("--form", default="auto")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--batch", type=int, default=0, help="use only the first N arrays of the workload")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -294,6 +295,8 @@ def main():
     if args.workload == "ragged":
         return run_ragged(args, wl, rank, world, local, dist, torch)
     xh = wl["x"]
+    if args.batch:
+        xh = np.ascontiguousarray(xh[:args.batch])
     b, h, w = xh.shape
     mode = wl["mode"]
     bytes_step = 8.0 * b * h * w

@@ -56,8 +56,12 @@ double sj_scale(int n, int k) {
 }
 
 // Four-step tables for N = 32 G (see sj_lines.cuh): twiddles w_N^{bc} s(32,c) and the
-// post-rotation coefficients with s(G,d) and the orthonormal factor folded in.  Fills
-// caller-provided arrays of G*17 float2 and 17*G float4.
+// post-rotation coefficients with the stage-2 SJ scale of each column and the orthonormal
+// factor folded in.  Stage 2 of column c produces V(d) / scale(c, d) with
+//   scale = s(G, d)          columns 1..15 when G < 32 (SJ scaled complex FFT),
+//           s(16, d >> 1)    columns 1..15 when G = 32 (split into two radix-2 halves),
+//           1                columns 0 and 16 (cooperative shuffle DFT across the lanes).
+// Fills caller-provided arrays of G*17 float2 (tw[b*17+c]) and G*17 float4 (post[d*17+c]).
 void fill_fourstep_tables(int N, float2* tw, float4* post) {
   const int G = N / 32;
   for (int b = 0; b < G; ++b)
@@ -70,13 +74,14 @@ void fill_fourstep_tables(int N, float2* tw, float4* post) {
   for (int c = 0; c < 17; ++c)
     for (int d = 0; d < G; ++d) {
       const int k = c + 32 * d;
-      const double th = M_PI * k / (2.0 * N), sg = sj_scale(G, d);
+      const double th = M_PI * k / (2.0 * N);
+      const double sg = (c == 0 || c == 16) ? 1.0 : G == 32 ? sj_scale(16, d >> 1) : sj_scale(G, d);
       float4 p;
       p.x = (float)(sig(k) * sg * std::cos(th));
       p.y = (float)(sig(k) * sg * std::sin(th));
       p.z = k ? (float)(sig(N - k) * sg * std::sin(th)) : 0.f;
       p.w = k ? (float)(-sig(N - k) * sg * std::cos(th)) : 0.f;
-      post[(size_t)c * G + d] = p;
+      post[(size_t)d * 17 + c] = p;
     }
 }
 

@@ -519,6 +519,30 @@ def build_cfft(n: int):
     return (g, outs), (gt, back)
 
 
+def build_cfft_half(n: int, half: int):
+    """One radix-2 DIF half of a complex FFT of length n (G = 32 stage-2 columns split across
+    two lanes): half 0 gives V(2m), half 1 gives V(2m+1), m = 0..n/2-1, each scaled by
+    1/s(n/2, m) (an SJ scaled FFT of length n/2 on the folded inputs)."""
+    m = n // 2
+
+    def prog(g, zs):
+        if half == 0:
+            folded = [g.cadd(zs[b], zs[b + m]) for b in range(m)]
+        else:
+            folded = [g.cmulc(g.csub(zs[b], zs[b + m]),
+                              complex(math.cos(2 * math.pi * b / n), -math.sin(2 * math.pi * b / n)))
+                      for b in range(m)]
+        z = cfft(g, folded, "S")
+        return [c for k in range(m) for c in z[k]]
+    g = Graph()
+    outs = prog(g, [(g.inp(2 * i), g.inp(2 * i + 1)) for i in range(n)])
+    gt = Graph()
+    outs_t = prog(gt, [(gt.inp(n + 2 * i), gt.inp(n + 2 * i + 1)) for i in range(n)])
+    adj = [gt.inp(i) for i in range(n)]
+    back = transpose(gt, outs_t, 3 * n, adj)[n:]
+    return (g, outs), (gt, back)
+
+
 def generate() -> str:
     parts = [
         "// Generated by gen_sj.py: Shao-Johnson scaled split-radix arithmetic (straight line).",
@@ -550,6 +574,16 @@ def generate() -> str:
                                f"const float (&w)[{m}], float (&x)[{LEAF}]",
                                f"transpose of sj_rfft_{LEAF}"))
     parts.append("")
+    for half in (0, 1):
+        (g, outs), (gt, back) = build_cfft_half(32, half)
+        parts.append(emit_function(g, f"sj_cfft_32_half{half}", [f"z[{i}]" for i in range(64)], outs,
+                                   [f"o[{i}]" for i in range(32)], "const float (&z)[64], float (&o)[32]",
+                                   f"DIF half {half} of the complex FFT of length 32"))
+        parts.append("")
+        parts.append(emit_function(gt, f"sj_cfft_32_half{half}_t", [f"o[{i}]" for i in range(32)] + ["0.0f"] * 64,
+                                   back, [f"z[{i}]" for i in range(64)], "const float (&o)[32], float (&z)[64]",
+                                   f"transpose of sj_cfft_32_half{half}"))
+        parts.append("")
     for n in STAGE2_SIZES:
         (g, outs), (gt, back) = build_cfft(n)
         parts.append(emit_function(g, f"sj_cfft_{n}", [f"z[{i}]" for i in range(2 * n)], outs,
@@ -609,6 +643,17 @@ def self_check() -> None:
         aty = gt.evaluate(back, np.concatenate([yv, np.zeros((2 * n, 1))]))
         assert abs(ax @ yv[:, 0] - flat[:, 0] @ aty[:, 0]) < 1e-9
         print(f"cfft N={n}: ops {g.count_ops(outs)}")
+    for half in (0, 1):
+        (g, outs), (gt, back) = build_cfft_half(32, half)
+        z = rng.standard_normal(32) + 1j * rng.standard_normal(32)
+        flat = np.stack([z.real, z.imag], 1).reshape(-1, 1)
+        got = g.evaluate(outs, flat).reshape(16, 2)
+        f = np.fft.fft(z)[half::2] / np.array([sj_scale(16, k) for k in range(16)])
+        assert np.abs(got[:, 0] + 1j * got[:, 1] - f).max() < 1e-10
+        yv = rng.standard_normal((32, 1))
+        aty = gt.evaluate(back, np.concatenate([yv, np.zeros((64, 1))]))
+        assert abs(got.reshape(-1) @ yv[:, 0] - flat[:, 0] @ aty[:, 0]) < 1e-9
+        print(f"cfft32 half {half}: ops {g.count_ops(outs)}")
     (g, outs), (gt, back) = build_rfft_leaf(LEAF)
     x = rng.standard_normal((LEAF, 1))
     got = g.evaluate(outs, x)[:, 0]

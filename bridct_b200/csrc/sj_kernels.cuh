@@ -42,6 +42,71 @@ template <> struct ExchangeFloats<512> { static constexpr int value = FourStepSi
 template <> struct ExchangeFloats<1024> { static constexpr int value = FourStepSizes<32>::FLOATS; };
 
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int round4(int a) { return (a + 3) & ~3; }
+
+// Floats of one line length's four-step tables in shared memory (post first: float4 aligned).
+template <int N> struct TableFloats {
+  static constexpr int G = N / 32;
+  static constexpr int value = N >= 128 ? 17 * G * 4 + round4(17 * G * 2) : 0;
+};
+
+// Copies the four-step tables of line length N into shared memory at s (16-byte aligned);
+// returns tables that point there.  The caller synchronizes before first use.
+template <int N>
+__device__ __forceinline__ FourStepTables stage_tables(FourStepTables g, float* s) {
+  if constexpr (N < 128) {
+    return g;
+  } else {
+    constexpr int G = N / 32;
+    float4* post = reinterpret_cast<float4*>(s);
+    float2* tw = reinterpret_cast<float2*>(s + 17 * G * 4);
+    for (int i = threadIdx.x; i < 17 * G; i += blockDim.x) {
+      post[i] = __ldg(g.post + i);
+      tw[i] = __ldg(g.tw + i);
+    }
+    return FourStepTables{tw, post};
+  }
+}
+
+// Shared-memory row pitch (floats).  A 16-byte aligned pitch (w + 4) lets the tile be staged
+// with 128-bit accesses and costs no extra bank conflicts in the line walks, except for column
+// four-step lines with G >= 16 (h >= 512), whose stage-1 reads need an odd pitch (w + 1).
+__host__ __device__ constexpr bool odd_pitch(int h, bool has_col) { return has_col && h >= 512; }
+__host__ __device__ constexpr int pitch_of(int h, int w, bool has_col) { return odd_pitch(h, has_col) ? w + 1 : w + 4; }
+
+// Moves rows x cols floats between global memory (row pitch gp) and the tile (pitch P).
+template <int P>
+__device__ __forceinline__ void tile_load(const float* g, long long gp, int rows, int cols, float* tile,
+                                          int valid_rows) {
+  const int q = cols / 4;
+  for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
+    const int r = i / q, c = (i % q) * 4;
+    const float4 v = r < valid_rows ? __ldg(reinterpret_cast<const float4*>(g + r * gp + c))
+                                    : make_float4(0.f, 0.f, 0.f, 0.f);
+    float* d = tile + r * P + c;
+    if constexpr (P % 4 == 0) {
+      *reinterpret_cast<float4*>(d) = v;
+    } else {
+      d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+    }
+  }
+}
+
+template <int P>
+__device__ __forceinline__ void tile_store(float* g, long long gp, int rows, int cols, const float* tile) {
+  const int q = cols / 4;
+  for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
+    const int r = i / q, c = (i % q) * 4;
+    const float* sp = tile + r * P + c;
+    float4 v;
+    if constexpr (P % 4 == 0) {
+      v = *reinterpret_cast<const float4*>(sp);
+    } else {
+      v = make_float4(sp[0], sp[1], sp[2], sp[3]);
+    }
+    *reinterpret_cast<float4*>(g + r * gp + c) = v;
+  }
+}
 
 // Runs all lines of length N in a set of `nlines` lines; line l starts at tile + off(l),
 // elements at stride es.  Register lines for N <= 64, warp four-step lines above.
@@ -66,41 +131,32 @@ __device__ __forceinline__ void run_lines(float* tile, int nlines, int es, const
 // matrix.  With DO_COL the tile holds TR/H whole arrays.
 template <int H, int W, int TR, bool DO_COL, bool DO_ROW, int MODE>
 __global__ void __launch_bounds__(kThreads) k_full(TileArgs a) {
-  constexpr int P = W + 1;
+  constexpr int P = pitch_of(H, W, DO_COL);
+  constexpr int XB = kWarps * cmax(DO_COL ? ExchangeFloats<H>::value : 0, DO_ROW ? ExchangeFloats<W>::value : 0);
   extern __shared__ float smem[];
   float* tile = smem;
-  float* xbuf = smem + TR * P;
-  constexpr int N4 = TR * W / 4;
+  float* xbuf = smem + round4(TR * P);
+  float* tabs = xbuf + round4(XB);
+  const FourStepTables tcol = DO_COL ? stage_tables<H>(a.tab.col, tabs) : a.tab.col;
+  const FourStepTables trow = DO_ROW ? stage_tables<W>(a.tab.row, tabs + (DO_COL ? TableFloats<H>::value : 0))
+                                     : a.tab.row;
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    const float4* src = reinterpret_cast<const float4*>(a.x + t * (long long)TR * W);
     // The last tile of a launch may hold fewer than TR rows; it is zero-filled.
     const long long left = a.rows_total - t * (long long)TR;
-    const int n4 = left >= TR ? N4 : (int)left * (W / 4);
-#pragma unroll 4
-    for (int i = threadIdx.x; i < N4; i += kThreads) {
-      const float4 v = i < n4 ? __ldg(src + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-      const int r = (4 * i) / W, c = (4 * i) % W;
-      float* d = tile + r * P + c;
-      d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-    }
+    const int rows = left >= TR ? TR : (int)left;
+    tile_load<P>(a.x + t * (long long)TR * W, W, TR, W, tile, rows);
     __syncthreads();
     if constexpr (DO_COL) {
       static_assert(TR % H == 0, "column pass needs whole arrays");
       run_lines<H, MODE>(tile, (TR / H) * W, P,
-                         [](int l) { return (l / W) * H * P + (l % W); }, xbuf, a.tab.col);
+                         [](int l) { return (l / W) * H * P + (l % W); }, xbuf, tcol);
       __syncthreads();
     }
     if constexpr (DO_ROW) {
-      run_lines<W, MODE>(tile, TR, 1, [](int l) { return l * P; }, xbuf, a.tab.row);
+      run_lines<W, MODE>(tile, TR, 1, [](int l) { return l * P; }, xbuf, trow);
       __syncthreads();
     }
-    float4* dst = reinterpret_cast<float4*>(a.y + t * (long long)TR * W);
-#pragma unroll 4
-    for (int i = threadIdx.x; i < n4; i += kThreads) {
-      const int r = (4 * i) / W, c = (4 * i) % W;
-      const float* s = tile + r * P + c;
-      dst[i] = make_float4(s[0], s[1], s[2], s[3]);
-    }
+    tile_store<P>(a.y + t * (long long)TR * W, W, rows, W, tile);
     __syncthreads();
   }
 }
@@ -108,51 +164,69 @@ __global__ void __launch_bounds__(kThreads) k_full(TileArgs a) {
 // Column strips: H rows x TC columns of one array (row pitch W in global memory).
 template <int H, int W, int TC, int MODE>
 __global__ void __launch_bounds__(kThreads) k_colstrip(TileArgs a) {
-  constexpr int P = TC + 1;
+  constexpr int P = pitch_of(H, TC, true);
   constexpr int STRIPS = W / TC;
-  constexpr int Q = TC / 4;   // float4 per strip row
   extern __shared__ float smem[];
   float* tile = smem;
-  float* xbuf = smem + H * P;
+  float* xbuf = smem + round4(H * P);
+  const FourStepTables tcol = stage_tables<H>(a.tab.col, xbuf + round4(kWarps * ExchangeFloats<H>::value));
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const long long arr = t / STRIPS;
     const int s = (int)(t % STRIPS);
-    const float* base = a.x + arr * (long long)H * W + s * TC;
-#pragma unroll 4
-    for (int i = threadIdx.x; i < H * Q; i += kThreads) {
-      const int r = i / Q, c = (i % Q) * 4;
-      const float4 v = __ldg(reinterpret_cast<const float4*>(base + (long long)r * W + c));
-      float* d = tile + r * P + c;
-      d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-    }
+    tile_load<P>(a.x + arr * (long long)H * W + s * TC, W, H, TC, tile, H);
     __syncthreads();
-    run_lines<H, MODE>(tile, TC, P, [](int l) { return l; }, xbuf, a.tab.col);
+    run_lines<H, MODE>(tile, TC, P, [](int l) { return l; }, xbuf, tcol);
     __syncthreads();
-    float* obase = a.y + arr * (long long)H * W + s * TC;
-#pragma unroll 4
-    for (int i = threadIdx.x; i < H * Q; i += kThreads) {
-      const int r = i / Q, c = (i % Q) * 4;
-      const float* sp = tile + r * P + c;
-      *reinterpret_cast<float4*>(obase + (long long)r * W + c) = make_float4(sp[0], sp[1], sp[2], sp[3]);
-    }
+    tile_store<P>(a.y + arr * (long long)H * W + s * TC, W, H, TC, tile);
     __syncthreads();
   }
 }
 
-// Compile-time launch geometry of one (H, W) shape.
+// Compile-time launch geometry of one (H, W) shape.  Shared-memory sizes are kept at or below
+// kSmemTwoPerSM so that two CTAs share an SM: tile rows (whole arrays), strip widths and row
+// blocks are halved from their targets until they fit.
+constexpr int kSmemTwoPerSM = 115712;
+
+template <int N> __host__ __device__ constexpr int lines_per_warp() { return N >= 128 ? 1024 / N : 1; }
+
 template <int H, int W>
 struct Geometry {
   static constexpr bool kTile = H * W <= 16384;
   // tile class
-  static constexpr int kArrays = cmax(1, kTileFloats / (H * W));
-  static constexpr int kTR = kTile ? kArrays * H : 1;
   static constexpr int kXbufFull = kWarps * cmax(ExchangeFloats<H>::value, ExchangeFloats<W>::value);
-  static constexpr int kSmemFull = (kTR * (W + 1) + kXbufFull) * 4;
+  static constexpr int full_smem(int arrays) {
+    return (round4(arrays * H * pitch_of(H, W, true)) + round4(kXbufFull) + TableFloats<H>::value +
+            TableFloats<W>::value) * 4;
+  }
+  static constexpr int pick_arrays() {
+    int a = cmax(1, kTileFloats / (H * W));
+    while (a > 1 && full_smem(a) > kSmemTwoPerSM) a /= 2;
+    return a;
+  }
+  static constexpr int kArrays = pick_arrays();
+  static constexpr int kTR = kTile ? kArrays * H : 1;
+  static constexpr int kSmemFull = full_smem(kArrays);
   // 2-pass class
-  static constexpr int kTC = (16384 / H) < W ? (16384 / H) : W;
-  static constexpr int kSmemStrip = (H * (kTC + 1) + kWarps * ExchangeFloats<H>::value) * 4;
-  static constexpr int kRB = cmax(1, 16384 / W);
-  static constexpr int kSmemRows = (kRB * (W + 1) + kWarps * ExchangeFloats<W>::value) * 4;
+  static constexpr int strip_smem(int tc) {
+    return (round4(H * pitch_of(H, tc, true)) + round4(kWarps * ExchangeFloats<H>::value) + TableFloats<H>::value) * 4;
+  }
+  static constexpr int pick_tc() {
+    int tc = (16384 / H) < W ? (16384 / H) : W;
+    while (tc > cmax(4, lines_per_warp<H>()) && strip_smem(tc) > kSmemTwoPerSM) tc /= 2;
+    return tc;
+  }
+  static constexpr int kTC = pick_tc();
+  static constexpr int kSmemStrip = strip_smem(kTC);
+  static constexpr int rows_smem(int rb) {
+    return (round4(rb * (W + 4)) + round4(kWarps * ExchangeFloats<W>::value) + TableFloats<W>::value) * 4;
+  }
+  static constexpr int pick_rb() {
+    int rb = cmax(1, 16384 / W);
+    while (rb > lines_per_warp<W>() && rows_smem(rb) > kSmemTwoPerSM) rb /= 2;
+    return rb;
+  }
+  static constexpr int kRB = pick_rb();
+  static constexpr int kSmemRows = rows_smem(kRB);
 };
 
 }  // namespace bridct

@@ -79,10 +79,15 @@ BRIDCT_CFFT(16)
 BRIDCT_CFFT(32)
 #undef BRIDCT_CFFT
 
-// Tables of one line length N (device memory, built on the host in float64):
-//   tw[b * 17 + c]   = w_N^{b c} s(32, c)                     (float2)
-//   post[c * G + d]  = (A, B, C, D) for k = c + 32 d          (float4)
-//     y[k] = A Vr + B Vi,  y[N-k] = C Vr + D Vi,  V = stage-2 output (scaled).
+// Tables of one line length N (built on the host in float64; the fixed-shape kernels copy them
+// into shared memory at start):
+//   tw[b * 17 + c]   = w_N^{b c} s(32, c)  for c = 1..15 (c = 0 and 16 need none:
+//                       s(32, 0) = s(32, 16) = 1 and column 16's rotation is inside sj_col16)
+//   post[d * 17 + c] = (A, B, C, D) for k = c + 32 d (d-major, so the lanes of a stage-2 round,
+//                       which hold consecutive columns c, read consecutive float4s):
+//     y[k] = A Vr + B Vi,  y[N-k] = C Vr + D Vi, with V the stage-2 output of column c, whose
+//     SJ scale (s(G,d); s(16,d>>1) for the split G = 32 columns; 1 for columns 0 and 16, which
+//     use an unscaled cooperative DFT) and the orthonormal factor are folded in.
 struct FourStepTables {
   const float2* tw;
   const float4* post;
@@ -93,7 +98,10 @@ template <int G>
 struct FourStepSizes {
   static constexpr int LPW = 32 / G;           // lines per warp
   static constexpr int PITCH = G + 1;          // odd pitch: conflict-free column reads
-  static constexpr int PLANE = LPW * 17 * PITCH;
+  // per-line stride: padded for G = 8, 16 so that the LPW lines' stage-1 writes hit disjoint
+  // banks (stride == G * odd mod 32); G = 4 stays unpadded to keep the 8-line buffer small
+  static constexpr int LINE = G == 8 ? 168 : G == 16 ? 304 : 17 * PITCH;
+  static constexpr int PLANE = LPW * LINE;
   static constexpr int FLOATS = 2 * PLANE;
 };
 
@@ -101,8 +109,85 @@ __device__ __forceinline__ int makhoul_src(int n, int N) {
   return n < N / 2 ? 2 * n : 2 * N - 1 - 2 * n;
 }
 
+// Cooperative DFT of length G across the G lanes of one line group (lane b holds element b):
+// radix-2 decimation in frequency with shuffles; on return lane b holds X(bitrev(b)).  The
+// twiddle w_G^m is tw[2m * 17 + 16] = w_N^{32 m} (table entry of column 16).
+template <int G>
+__device__ __forceinline__ void coop_dft(float& re, float& im, int b, const float2* tw) {
+#pragma unroll
+  for (int s = G / 2; s >= 1; s >>= 1) {
+    const float pr = __shfl_xor_sync(0xFFFFFFFFu, re, s, G);
+    const float pi = __shfl_xor_sync(0xFFFFFFFFu, im, s, G);
+    if (b & s) {
+      const float2 w = tw[(2 * (b & (s - 1)) * (G / (2 * s))) * 17 + 16];
+      const float dr = pr - re, di = pi - im;
+      re = dr * w.x - di * w.y;
+      im = dr * w.y + di * w.x;
+    } else {
+      re += pr;
+      im += pi;
+    }
+  }
+}
+
+// Transpose of coop_dft: lane b holds the adjoint of X(bitrev(b)) on entry and of x_b on return.
+template <int G>
+__device__ __forceinline__ void coop_dft_t(float& re, float& im, int b, const float2* tw) {
+#pragma unroll
+  for (int s = 1; s <= G / 2; s <<= 1) {
+    const float pr = __shfl_xor_sync(0xFFFFFFFFu, re, s, G);
+    const float pi = __shfl_xor_sync(0xFFFFFFFFu, im, s, G);
+    const float2 w = tw[(2 * (b & (s - 1)) * (G / (2 * s))) * 17 + 16];
+    if (b & s) {                      // x_{j+s} = top - conj(w) * bottom
+      const float nr = pr - (re * w.x + im * w.y);
+      const float ni = pi - (im * w.x - re * w.y);
+      re = nr;
+      im = ni;
+    } else {                          // x_j = top + conj(w) * bottom
+      re = re + (pr * w.x + pi * w.y);
+      im = im + (pi * w.x - pr * w.y);
+    }
+  }
+}
+
+template <int G>
+__device__ __forceinline__ int bitrev(int b) {
+  return (int)(__brev((unsigned)b) >> (32 - __ffs(G) + 1));
+}
+
+// Post rotation of one stage-2 output V(d) of column c into the line (and its transpose).
+__device__ __forceinline__ void post_store(float* line, int es, int N, int k, float4 p, float vr, float vi) {
+  if (k == 0) {
+    line[0] = p.x * vr;
+  } else {
+    line[k * es] = p.x * vr + p.y * vi;
+    if (2 * k != N) line[(N - k) * es] = p.z * vr + p.w * vi;
+  }
+}
+__device__ __forceinline__ void post_load(const float* line, int es, int N, int k, float4 p, float& vr, float& vi) {
+  if (k == 0) {
+    vr = p.x * line[0];
+    vi = 0.0f;
+  } else {
+    const float yk = line[k * es];
+    vr = p.x * yk;
+    vi = p.y * yk;
+    if (2 * k != N) {
+      const float ynk = line[(N - k) * es];
+      vr += p.z * ynk;
+      vi += p.w * ynk;
+    }
+  }
+}
+
 // Forward four-step on the LPW lines owned by this warp.  line_ptr(j) returns the base of
 // the warp's j-th line (j < LPW); es = element stride.  xb = this warp's exchange buffer.
+//   stage 1   lane b: SJ real FFT of length 32 of v[G a + b]; columns c = 1..15 twiddled into
+//             the exchange buffer; columns 0 and 16 stay in registers
+//   special   columns 0 and 16: cooperative shuffle DFT over the line's G lanes (column 16
+//             pre-rotated by w_N^{16 b}); lane b stores V(bitrev(b)) where that index is needed
+//   stage 2   columns 1..15: generated SJ complex FFT of length G per task (G = 32: each column
+//             split into its two radix-2 halves, so 30 lanes do equal work)
 template <int G, typename LinePtr>
 __device__ __forceinline__ void fs_forward(const LinePtr& line_ptr, int es, float* xb,
                                            FourStepTables tab) {
@@ -110,55 +195,73 @@ __device__ __forceinline__ void fs_forward(const LinePtr& line_ptr, int es, floa
   using SZ = FourStepSizes<G>;
   const int lane = threadIdx.x & 31;
   const int grp = lane / G, b = lane % G;
+  float w0, w16;
   {
     float* line = line_ptr(grp);
     float xin[32], w[32];
 #pragma unroll
     for (int a = 0; a < 32; ++a) xin[a] = line[makhoul_src(G * a + b, N) * es];
     sj_rfft_32(xin, w);
-    float* re = xb + grp * 17 * SZ::PITCH + b;
+    float* re = xb + grp * SZ::LINE + b;
     float* im = re + SZ::PLANE;
-    re[0] = w[0];
-    im[0] = 0.0f;
 #pragma unroll
     for (int c = 1; c < 16; ++c) {
-      const float2 t = __ldg(&tab.tw[b * 17 + c]);
+      const float2 t = tab.tw[b * 17 + c];
       const float wr = w[c], wi = w[16 + c];
       re[c * SZ::PITCH] = wr * t.x - wi * t.y;
       im[c * SZ::PITCH] = wr * t.y + wi * t.x;
     }
-    {
-      const float2 t = __ldg(&tab.tw[b * 17 + 16]);
-      re[16 * SZ::PITCH] = w[16] * t.x;
-      im[16 * SZ::PITCH] = w[16] * t.y;
-    }
+    w0 = w[0];
+    w16 = w[16];
   }
-  __syncwarp();
-  for (int task = lane; task < SZ::LPW * 17; task += 32) {
-    const int g2 = task / 17, c = task % 17;
-    const float* re = xb + task * SZ::PITCH;
-    const float* im = re + SZ::PLANE;
-    float z[2 * G];
+  // columns 0 and 16 (all lanes, registers and shuffles)
+  float ar = w0, ai = 0.0f;
+  coop_dft<G>(ar, ai, b, tab.tw);
+  const float2 rot = tab.tw[b * 17 + 16];
+  float cr = w16 * rot.x, ci = w16 * rot.y;
+  coop_dft<G>(cr, ci, b, tab.tw);
+  __syncwarp();                                  // every lane has read its stage-1 inputs
+  {
+    float* line = line_ptr(grp);
+    const int d = bitrev<G>(b);
+    if (d <= G / 2) post_store(line, es, N, 32 * d, tab.post[d * 17], ar, (d == 0 || d == G / 2) ? 0.0f : ai);
+    if (d < G / 2) post_store(line, es, N, 16 + 32 * d, tab.post[d * 17 + 16], cr, ci);
+  }
+  if constexpr (G == 32) {
+    if (lane < 30) {
+      float* line = line_ptr(0);
+      const float* re = xb;
+      const float* im = xb + SZ::PLANE;
+      const int c = 1 + (lane >> 1), h = lane & 1;
+      float z[64], o[32];
 #pragma unroll
-    for (int q = 0; q < G; ++q) {
-      z[2 * q] = re[q];
-      z[2 * q + 1] = im[q];
-    }
-    CFFT<G>::fwd(z);
-    float* line = line_ptr(g2);
-    const int dmax = (c == 0) ? G / 2 : (c == 16 ? G / 2 - 1 : G - 1);
-#pragma unroll
-    for (int d = 0; d < G; ++d) {
-      if (d > dmax) break;
-      const int k = c + 32 * d;
-      const float4 p = __ldg(&tab.post[c * G + d]);
-      const float vr = z[2 * d], vi = z[2 * d + 1];
-      if (k == 0) {
-        line[0] = p.x * vr;
-      } else {
-        line[k * es] = p.x * vr + p.y * vi;
-        if (2 * k != N) line[(N - k) * es] = p.z * vr + p.w * vi;
+      for (int q = 0; q < 32; ++q) {
+        z[2 * q] = re[c * SZ::PITCH + q];
+        z[2 * q + 1] = im[c * SZ::PITCH + q];
       }
+      if (h) sj_cfft_32_half1(z, o);
+      else sj_cfft_32_half0(z, o);
+#pragma unroll
+      for (int m = 0; m < 16; ++m) {
+        const int dd = 2 * m + h;
+        post_store(line, es, N, c + 32 * dd, tab.post[dd * 17 + c], o[2 * m], o[2 * m + 1]);
+      }
+    }
+  } else {
+    for (int task = lane; task < SZ::LPW * 15; task += 32) {
+      const int g2 = task / 15, c = 1 + task % 15;
+      float* line = line_ptr(g2);
+      const float* re = xb + g2 * SZ::LINE + c * SZ::PITCH;
+      const float* im = re + SZ::PLANE;
+      float z[2 * G];
+#pragma unroll
+      for (int q = 0; q < G; ++q) {
+        z[2 * q] = re[q];
+        z[2 * q + 1] = im[q];
+      }
+      CFFT<G>::fwd(z);
+#pragma unroll
+      for (int dd = 0; dd < G; ++dd) post_store(line, es, N, c + 32 * dd, tab.post[dd * 17 + c], z[2 * dd], z[2 * dd + 1]);
     }
   }
   __syncwarp();
@@ -171,60 +274,78 @@ __device__ __forceinline__ void fs_inverse(const LinePtr& line_ptr, int es, floa
   constexpr int N = 32 * G;
   using SZ = FourStepSizes<G>;
   const int lane = threadIdx.x & 31;
-  for (int task = lane; task < SZ::LPW * 17; task += 32) {
-    const int g2 = task / 17, c = task % 17;
-    const float* line = line_ptr(g2);
-    const int dmax = (c == 0) ? G / 2 : (c == 16 ? G / 2 - 1 : G - 1);
-    float z[2 * G];
-#pragma unroll
-    for (int d = 0; d < G; ++d) {
-      float zr = 0.0f, zi = 0.0f;
-      if (d <= dmax) {
-        const int k = c + 32 * d;
-        const float4 p = __ldg(&tab.post[c * G + d]);
-        if (k == 0) {
-          zr = p.x * line[0];
-        } else {
-          const float yk = line[k * es];
-          zr = p.x * yk;
-          zi = p.y * yk;
-          if (2 * k != N) {
-            const float ynk = line[(N - k) * es];
-            zr += p.z * ynk;
-            zi += p.w * ynk;
-          }
-        }
-      }
-      z[2 * d] = zr;
-      z[2 * d + 1] = zi;
+  const int grp = lane / G, b = lane % G;
+  // columns 0 and 16: adjoints of V(bitrev(b)), then the transposed cooperative DFTs
+  float ar = 0.0f, ai = 0.0f, cr = 0.0f, ci = 0.0f;
+  {
+    const float* line = line_ptr(grp);
+    const int d = bitrev<G>(b);
+    if (d <= G / 2) {
+      post_load(line, es, N, 32 * d, tab.post[d * 17], ar, ai);
+      if (d == 0 || d == G / 2) ai = 0.0f;
     }
-    CFFT<G>::tr(z);
-    float* re = xb + task * SZ::PITCH;
-    float* im = re + SZ::PLANE;
+    if (d < G / 2) post_load(line, es, N, 16 + 32 * d, tab.post[d * 17 + 16], cr, ci);
+  }
+  coop_dft_t<G>(ar, ai, b, tab.tw);
+  coop_dft_t<G>(cr, ci, b, tab.tw);
+  const float2 rot = tab.tw[b * 17 + 16];
+  const float w0 = ar;                           // real part: the forward input was real
+  const float w16 = cr * rot.x + ci * rot.y;     // Re(conj(rotation) * adjoint)
+  if constexpr (G == 32) {
+    if (lane < 30) {
+      const float* line = line_ptr(0);
+      float* re = xb;
+      float* im = xb + SZ::PLANE;
+      const int c = 1 + (lane >> 1), h = lane & 1;
+      float o[32], z[64];
 #pragma unroll
-    for (int q = 0; q < G; ++q) {
-      re[q] = z[2 * q];
-      im[q] = z[2 * q + 1];
+      for (int m = 0; m < 16; ++m) {
+        const int dd = 2 * m + h;
+        post_load(line, es, N, c + 32 * dd, tab.post[dd * 17 + c], o[2 * m], o[2 * m + 1]);
+      }
+      if (h) sj_cfft_32_half1_t(o, z);
+      else sj_cfft_32_half0_t(o, z);
+      // both halves feed every b: each lane sums one half of the b range with its partner
+#pragma unroll
+      for (int q = 0; q < 32; ++q) {
+        const float send = h ? z[q] : z[32 + q];
+        const float recv = __shfl_xor_sync(0x3FFFFFFFu, send, 1);
+        const float sum = (h ? z[32 + q] : z[q]) + recv;
+        const int bb = (h ? 16 : 0) + (q >> 1);
+        ((q & 1) ? im : re)[c * SZ::PITCH + bb] = sum;
+      }
+    }
+  } else {
+    for (int task = lane; task < SZ::LPW * 15; task += 32) {
+      const int g2 = task / 15, c = 1 + task % 15;
+      const float* line = line_ptr(g2);
+      float* re = xb + g2 * SZ::LINE + c * SZ::PITCH;
+      float* im = re + SZ::PLANE;
+      float z[2 * G];
+#pragma unroll
+      for (int dd = 0; dd < G; ++dd) post_load(line, es, N, c + 32 * dd, tab.post[dd * 17 + c], z[2 * dd], z[2 * dd + 1]);
+      CFFT<G>::tr(z);
+#pragma unroll
+      for (int q = 0; q < G; ++q) {
+        re[q] = z[2 * q];
+        im[q] = z[2 * q + 1];
+      }
     }
   }
   __syncwarp();
   {
-    const int grp = lane / G, b = lane % G;
-    const float* re = xb + grp * 17 * SZ::PITCH + b;
+    const float* re = xb + grp * SZ::LINE + b;
     const float* im = re + SZ::PLANE;
     float w[32], xo[32];
-    w[0] = re[0];
+    w[0] = w0;
 #pragma unroll
     for (int c = 1; c < 16; ++c) {
-      const float2 t = __ldg(&tab.tw[b * 17 + c]);
+      const float2 t = tab.tw[b * 17 + c];
       const float tr = re[c * SZ::PITCH], ti = im[c * SZ::PITCH];
       w[c] = tr * t.x + ti * t.y;
       w[16 + c] = ti * t.x - tr * t.y;
     }
-    {
-      const float2 t = __ldg(&tab.tw[b * 17 + 16]);
-      w[16] = re[16 * SZ::PITCH] * t.x + im[16 * SZ::PITCH] * t.y;
-    }
+    w[16] = w16;
     sj_rfft_32_t(w, xo);
     float* line = line_ptr(grp);
 #pragma unroll
