@@ -50,11 +50,25 @@ template <int MODE>
 __global__ void __launch_bounds__(kB8Threads) k_blocks8(const float* __restrict__ x,
                                                         float* __restrict__ y, long long batch) {
   extern __shared__ float4 s8[];
-  const long long ntiles = (batch + kB8Threads - 1) / kB8Threads;
+  // Full rounds: tile r*grid + blockIdx of 256 arrays (all CTAs stream one contiguous region
+  // together).  The arrays left after the full rounds are split evenly over all CTAs (fewer
+  // than 256 each), so the launch has no tail round in which a fraction of the SMs works alone.
+  const long long round_arrays = (long long)gridDim.x * kB8Threads;
+  const long long full = batch / round_arrays;
+  const long long rest = batch - full * round_arrays;
+  const long long per = rest / gridDim.x, extra = rest % gridDim.x;
   const int t = threadIdx.x;
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long long first = tile * kB8Threads;
-    const int arrays = batch - first < kB8Threads ? (int)(batch - first) : kB8Threads;
+  for (long long round = 0; round <= full; ++round) {
+    long long first;
+    int arrays;
+    if (round < full) {
+      first = round * round_arrays + (long long)blockIdx.x * kB8Threads;
+      arrays = kB8Threads;
+    } else {
+      first = full * round_arrays + blockIdx.x * per + (blockIdx.x < extra ? blockIdx.x : extra);
+      arrays = (int)(per + (blockIdx.x < extra ? 1 : 0));
+      if (arrays == 0) break;
+    }
     const int chunks = arrays * 16;
     const float4* src = reinterpret_cast<const float4*>(x) + first * 16;
     float4 buf[16];

@@ -5,17 +5,17 @@
 // tile of 128 arrays stored contiguously (128 rows of 64 floats) this is one GEMM
 //     Y_tile (128 x 64) = X_tile (128 x 64) . K^T (64 x 64)
 // i.e. tcgen05.mma with M = 128, N = 64, K = 64, A = X tile (K-major), B = K (K-major),
-// D = FP32 accumulator in 64 TMEM columns.  Split precision keeps FP32 accuracy:
-//   BF16x3: X = Xh + Xm + Xl and K = Kh + Km + Kl (bf16 each); six products
-//           Xl Kh + Xm Km + Xh Kl + Xm Kh + Xh Km + Xh Kh accumulate in FP32 (smallest first).
-//   TF32x3: X = Xh + Xl, K = Kh + Kl (tf32); three products Xl Kh + Xh Kl + Xh Kh.
+// D = FP32 accumulators in TMEM.  Split precision keeps FP32 accuracy:
+//   BF16x3: X = Xh + Xm + Xl (exact truncation split) and K = Kh + Km + Kl (bf16 each); six products
+//           Xh Kh + (Xh Km + Xm Kh + Xl Kh) + (Xh Kl + Xm Km), in three MMAs per K step.
+//   TF32x3: X = Xh + Xl, K = Kh + Kl (tf32); three products Xh Kh + (Xh Kl + Xl Kh), two MMAs.
 // K and its splits are computed in float64 on the host and uploaded once, already in the
 // shared-memory image the MMA reads (128-byte swizzled, K-major).
 //
 // The kernel is a persistent, warp-specialized pipeline (one CTA per SM): a TMA producer
 // fills a 4- or 5-deep ring of FP32 tiles (two 128x32 boxes each, 128-byte swizzle = exactly the
 // UMMA K-major SW128 layout), four split warps turn ring tiles into operand tiles, one thread
-// issues the MMAs into one of two TMEM accumulators, and four epilogue warps read the
+// issues the MMAs into one of two TMEM accumulator sets, and four epilogue warps read the
 // accumulator with tcgen05.ld (warp w owns TMEM lanes 32(w%4)..+31 = tile rows), write the
 // result swizzled back into the ring tile and TMA-store it.  Loads, splits, MMAs and stores of
 // consecutive tiles overlap.
@@ -34,7 +34,8 @@ namespace tc {
 
 constexpr int kRows = 128;          // arrays per tile (MMA M)
 constexpr int kCols = 64;           // elements per array (MMA N and K)
-constexpr int kTmemCols = 64;
+constexpr int kTmemCols = 192;      // per tile: [big | small | smaller] x 64 columns
+constexpr int kTmemAlloc = 512;    // two tiles, rounded up to a power of two
 constexpr uint32_t kSpinLimit = 1u << 26;   // bounded mbarrier polls (~seconds)
 
 enum Form { BF16X3 = 1, TF32X3 = 2 };
@@ -44,7 +45,7 @@ enum Form { BF16X3 = 1, TF32X3 = 2 };
 //   output tile for the TMA store), kABufs A-operand buffers (BF16: Xh|Xm|Xl, TF32: Xl),
 //   the B image, and the mbarriers.
 constexpr int kABufs = 2;
-constexpr int kAccs = 2;            // TMEM accumulators (64 columns each)
+constexpr int kAccs = 2;            // TMEM accumulator sets (kTmemCols columns each)
 constexpr int kTile = kRows * kCols * 4;   // FP32 tile bytes (32 KB)
 constexpr int kMaxStages = 5;
 
@@ -100,10 +101,9 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return d;
 }
 
-// Instruction descriptor: D FP32, A/B format fmt (1 = BF16, 2 = TF32), K-major, M=128, N=64.
-__host__ __device__ constexpr uint32_t instr_desc(uint32_t fmt) {
-  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(kCols >> 3) << 17) |
-         ((uint32_t)(kRows >> 4) << 24);
+// Instruction descriptor: D FP32, A/B format fmt (1 = BF16, 2 = TF32), K-major, M=128, N=n.
+__host__ __device__ constexpr uint32_t instr_desc(uint32_t fmt, uint32_t n = kCols) {
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((n >> 3) << 17) | ((uint32_t)(kRows >> 4) << 24);
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
@@ -213,22 +213,44 @@ __device__ __forceinline__ void named_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
+// Exact 3-way bf16 split of two FP32 values by truncation: hi = x with its low 16 bits cleared,
+// mid = (x - hi) likewise, lo = x - hi - mid.  Both subtractions are exact (same exponent, the
+// remaining significand bits), lo keeps at most 8 significant bits, so x = hi + mid + lo holds
+// exactly and every part is its FP32 value's upper 16 bits.  Returns the packed bf16 pairs
+// (first value in the low half).
+__device__ __forceinline__ void split_bf16x3_pair(float x0, float x1, uint32_t& hi, uint32_t& mid, uint32_t& lo) {
+  const uint32_t u0 = __float_as_uint(x0), u1 = __float_as_uint(x1);
+  const float r0 = x0 - __uint_as_float(u0 & 0xFFFF0000u), r1 = x1 - __uint_as_float(u1 & 0xFFFF0000u);
+  const uint32_t v0 = __float_as_uint(r0), v1 = __float_as_uint(r1);
+  const float q0 = r0 - __uint_as_float(v0 & 0xFFFF0000u), q1 = r1 - __uint_as_float(v1 & 0xFFFF0000u);
+  hi = __byte_perm(u0, u1, 0x7632);
+  mid = __byte_perm(v0, v1, 0x7632);
+  lo = __byte_perm(__float_as_uint(q0), __float_as_uint(q1), 0x7632);
+}
+
+// TF32 split of four values: Xh = x with its low 13 bits cleared (the tf32 the MMA reads),
+// Xl = rna_tf32(x - Xh).
+__device__ __forceinline__ void split_tf32x2(const float4& v, uint4& h, uint4& l) {
+  h = make_uint4(__float_as_uint(v.x) & 0xFFFFE000u, __float_as_uint(v.y) & 0xFFFFE000u,
+                 __float_as_uint(v.z) & 0xFFFFE000u, __float_as_uint(v.w) & 0xFFFFE000u);
+  l = make_uint4(tf32_rna(v.x - __uint_as_float(h.x)), tf32_rna(v.y - __uint_as_float(h.y)),
+                 tf32_rna(v.z - __uint_as_float(h.z)), tf32_rna(v.w - __uint_as_float(h.w)));
+}
+
 // Splits FP32 ring tile `stage` into A buffer `abuf` (thread r of 128 owns tile row r).
 template <int FORM>
 __device__ __forceinline__ void split_tile(uint8_t* stage, uint8_t* abuf, uint32_t r) {
   if constexpr (FORM == TF32X3) {
-    // elementwise: Xh = rna_tf32(X) in place, Xl = X - Xh into the A buffer (same layout)
+    // elementwise: Xh in place, Xl into the A buffer (same layout)
 #pragma unroll
     for (int box = 0; box < 2; ++box)
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const uint32_t off = box * 16384u + sw128(r, j);
-        const float4 v = *reinterpret_cast<const float4*>(stage + off);
-        const uint32_t h0 = tf32_rna(v.x), h1 = tf32_rna(v.y), h2 = tf32_rna(v.z), h3 = tf32_rna(v.w);
-        const float4 lo = make_float4(v.x - __uint_as_float(h0), v.y - __uint_as_float(h1),
-                                      v.z - __uint_as_float(h2), v.w - __uint_as_float(h3));
-        *reinterpret_cast<uint4*>(stage + off) = make_uint4(h0, h1, h2, h3);
-        *reinterpret_cast<float4*>(abuf + off) = lo;
+        uint4 h, l;
+        split_tf32x2(*reinterpret_cast<const float4*>(stage + off), h, l);
+        *reinterpret_cast<uint4*>(stage + off) = h;
+        *reinterpret_cast<uint4*>(abuf + off) = l;
       }
   } else {
     // Row r's 64 FP32 values (box 0 row r: elements 0..31, box 1 row r: 32..63) are read
@@ -244,20 +266,7 @@ __device__ __forceinline__ void split_tile(uint8_t* stage, uint8_t* abuf, uint32
     for (int jp = 0; jp < 8; ++jp) {
       uint32_t hi[4], mid[4], lo[4];
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        __nv_bfloat16 h[2], m[2], l[2];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const float v = x[8 * jp + 2 * e + q];
-          h[q] = __float2bfloat16_rn(v);
-          const float r1 = v - __bfloat162float(h[q]);
-          m[q] = __float2bfloat16_rn(r1);
-          l[q] = __float2bfloat16_rn(r1 - __bfloat162float(m[q]));
-        }
-        hi[e] = pack_bf16(h[0], h[1]);
-        mid[e] = pack_bf16(m[0], m[1]);
-        lo[e] = pack_bf16(l[0], l[1]);
-      }
+      for (int e = 0; e < 4; ++e) split_bf16x3_pair(x[8 * jp + 2 * e], x[8 * jp + 2 * e + 1], hi[e], mid[e], lo[e]);
       const uint32_t off = sw128(r, jp);
       *reinterpret_cast<uint4*>(stage + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
       *reinterpret_cast<uint4*>(stage + 16384u + off) = make_uint4(mid[0], mid[1], mid[2], mid[3]);
@@ -268,38 +277,34 @@ __device__ __forceinline__ void split_tile(uint8_t* stage, uint8_t* abuf, uint32
 
 // Issues the split-product MMAs of one tile (one thread).  sstage / sabuf / sb: shared
 // addresses of the ring tile, the A buffer and the B image.
+//
+// Products that share an A split go into one MMA with the B splits stacked along N (the B
+// image holds [Kh; Km; Kl] as 64-row blocks per 32- or 64-element K atom), so each A split is
+// read once per K step.  The accumulator set of a tile is [big | small | smaller] (64 columns
+// each): the dominant Xh.Kh product accumulates apart from the small products, whose own FP32
+// accumulation losses are then negligible, and the epilogue adds the three in FP32.
+//   BF16x3: Xh.[Kh|Km|Kl] -> [big|small|smaller], Xm.[Kh|Km] -> [small|smaller], Xl.Kh -> small
+//   TF32x3: Xh.[Kh|Kl]    -> [big|small],         Xl.Kh     -> small
 template <int FORM>
 __device__ __forceinline__ void issue_mmas(uint32_t sstage, uint32_t sabuf, uint32_t sb, uint32_t tmem_d) {
   if constexpr (FORM == BF16X3) {
-    // (A split, B split) products, smallest magnitude first: A = {Xh, Xm, Xl}, B = {Kh, Km, Kl};
-    // Xh and Xm sit in the ring tile's two boxes, Xl in the A buffer.
-    const uint32_t asplit[3] = {sstage, sstage + 16384u, sabuf};
-    constexpr int pa[6] = {2, 1, 0, 1, 0, 0};
-    constexpr int pb[6] = {0, 1, 2, 0, 1, 0};
-    constexpr uint32_t idesc = instr_desc(1);
+    constexpr uint32_t i192 = instr_desc(1, 192), i128 = instr_desc(1, 128), i64 = instr_desc(1, 64);
 #pragma unroll
-    for (int p = 0; p < 6; ++p)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {   // K = 16 bf16 = 32 bytes per MMA
-        const uint64_t ad = sw128_desc(asplit[pa[p]] + k * 32u);
-        const uint64_t bd = sw128_desc(sb + pb[p] * 8192u + k * 32u);
-        umma(tmem_d, ad, bd, idesc, (p | k) ? 1u : 0u, BF16X3);
-      }
+    for (int k = 0; k < 4; ++k) {   // K = 16 bf16 = 32 bytes per MMA
+      const uint64_t bd = sw128_desc(sb + k * 32u);
+      umma(tmem_d, sw128_desc(sstage + k * 32u), bd, i192, k ? 1u : 0u, BF16X3);
+      umma(tmem_d + 64, sw128_desc(sstage + 16384u + k * 32u), bd, i128, 1u, BF16X3);
+      umma(tmem_d + 64, sw128_desc(sabuf + k * 32u), bd, i64, 1u, BF16X3);
+    }
   } else {
-    // A = {Xl (A buffer), Xh (ring tile), Xh}, B = {Kh, Kl, Kh}: products Xl Kh, Xh Kl, Xh Kh
-    const uint32_t abase[3] = {sabuf, sstage, sstage};
-    constexpr int pb[3] = {0, 1, 0};
-    constexpr uint32_t idesc = instr_desc(2);
+    constexpr uint32_t i128 = instr_desc(2, 128), i64 = instr_desc(2, 64);
 #pragma unroll
-    for (int p = 0; p < 3; ++p)
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {   // K = 8 tf32 = 32 bytes per MMA; 32-element atoms
-        const uint32_t koff = (k >> 2) * 16384u + (k & 3) * 32u;
-        const uint32_t kboff = (k >> 2) * 8192u + (k & 3) * 32u;
-        const uint64_t ad = sw128_desc(abase[p] + koff);
-        const uint64_t bd = sw128_desc(sb + pb[p] * 16384u + kboff);
-        umma(tmem_d, ad, bd, idesc, (p | k) ? 1u : 0u, TF32X3);
-      }
+    for (int k = 0; k < 8; ++k) {   // K = 8 tf32 = 32 bytes per MMA; 32-element atoms
+      const uint32_t koff = (k >> 2) * 16384u + (k & 3) * 32u;
+      const uint64_t bd = sw128_desc(sb + (k >> 2) * 16384u + (k & 3) * 32u);
+      umma(tmem_d, sw128_desc(sstage + koff), bd, i128, k ? 1u : 0u, TF32X3);
+      umma(tmem_d + 64, sw128_desc(sabuf + koff), bd, i64, 1u, TF32X3);
+    }
   }
 }
 
@@ -360,7 +365,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_tc8(const __grid_constant__ C
   }
   if (warp == 2) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(kAccs * kTmemCols));
+                 "r"(kTmemAlloc));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   {
@@ -439,12 +444,21 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_tc8(const __grid_constant__ C
       const uint32_t taddr = tmem_base + t * kTmemCols + (quarter << 16);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        float w[16];
-        tmem_ld16(taddr + q * 16, w);
+        float big[16], sm[16];
+        tmem_ld16(taddr + q * 16, big);
+        tmem_ld16(taddr + 64 + q * 16, sm);
+        if constexpr (FORM == BF16X3) {
+          float sm2[16];
+          tmem_ld16(taddr + 128 + q * 16, sm2);
+          tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[q * 16 + i] = w[i];
+          for (int i = 0; i < 16; ++i) sm[i] += sm2[i];
+        } else {
+          tmem_wait_ld();
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[q * 16 + i] = big[i] + sm[i];
       }
-      tmem_wait_ld();
       tc_fence_before();
       named_sync(2, 128);
       if (r == 0) mbar_arrive(bars.acc_free + 8 * t);
@@ -476,7 +490,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_tc8(const __grid_constant__ C
   __syncthreads();
   tc_fence_after();
   if (warp == 2) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kAccs * kTmemCols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kTmemAlloc));
   }
 }
 

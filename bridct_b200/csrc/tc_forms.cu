@@ -1,10 +1,16 @@
-// Host side of the tensor-core precision forms (BRIDCT_FORM_TC_*), 8x8 arrays.
+// Host side of the tensor-core precision forms (BRIDCT_FORM_TC_*).
 //
-// The Kronecker matrix of the orthonormal 8x8 DCT-II (and its transpose for the inverse) is
+// 8x8 arrays: the Kronecker matrix of the orthonormal 8x8 DCT-II (and its transpose for the inverse) is
 // built in float64, split into bf16 (hi/mid/lo) or tf32 (hi/lo) parts and laid out as the
 // exact shared-memory image the UMMA B operand reads (K-major, 128-byte swizzle); the images
 // are uploaded once per device.  Each call encodes two TMA tensor maps (input and output
 // viewed as batch x 64 FP32 matrices, box 32 x 128, 128-byte swizzle) and launches k_tc8.
+//
+// Axes of 64, 128 and 256 (any combination): two row passes of k_tcpass per batch of arrays
+// (pass 1 over rows of length W into a plan-owned scratch, pass 2 over rows of length H into
+// the output), with the batch cut so that the scratch stays in L2 between the passes.  The B
+// images hold C_L (or C_L^T for the inverse) split into bf16 or tf32 parts, one 64-row slice
+// per N-block, in the K-major 128-byte-swizzled layout.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -18,6 +24,7 @@
 #include "../../include/bridct_b200.h"
 #include "bridct_internal.h"
 #include "tc_blocks8.cuh"
+#include "tc_pass.cuh"
 
 namespace bridct {
 namespace {
@@ -106,16 +113,63 @@ std::vector<uint8_t> b_image(int form, bool inverse) {
       const float h = tf32_round(v);
       const float l = tf32_round(v - h);
       const float parts[2] = {h, l};
-      const uint32_t off = (k / 32) * 8192 + tc::sw128(n, (k % 32) / 4) + (k % 4) * 4;
-      for (int s = 0; s < 2; ++s) memcpy(&img[s * 16384 + off], &parts[s], 4);
+      // per 32-element K atom: Kh rows then Kl rows (the N = 128 MMA reads both)
+      const uint32_t off = (k / 32) * 16384 + tc::sw128(n, (k % 32) / 4) + (k % 4) * 4;
+      for (int s = 0; s < 2; ++s) memcpy(&img[off + s * 8192], &parts[s], 4);
     }
   return img;
 }
 
 struct TcDevice {
   void* images[3][2] = {};   // [form][inverse]
+  void* pass_images[3][3][2] = {};   // [form][log2(L) - 6][inverse], built on first use
   int* err = nullptr;
 };
+
+// Orthonormal DCT-II matrix C_L[n][k] = sqrt((n ? 2 : 1) / L) cos(pi n (k + 1/2) / L).
+std::vector<double> dct_matrix(int L) {
+  std::vector<double> c((size_t)L * L);
+  for (int n = 0; n < L; ++n)
+    for (int k = 0; k < L; ++k)
+      c[(size_t)n * L + k] = std::sqrt((n ? 2.0 : 1.0) / L) * std::cos(M_PI * n * (k + 0.5) / L);
+  return c;
+}
+
+// B image of the row pass for rows of length L: slice nb (64 output columns) at nb * kBBytes,
+// laid out [K-chunk][split][8 KB atom column]; B[n][k] = C_L[n][k] (forward) or C_L[k][n].
+template <int FORM, int L>
+std::vector<uint8_t> pass_image(bool inverse) {
+  using PL = tc::PassLayout<FORM, L>;
+  constexpr int kc_len = tc::PassForm<FORM>::kKC;
+  const std::vector<double> c = dct_matrix(L);
+  std::vector<uint8_t> img((size_t)PL::kBlocks * PL::kBBytes, 0);
+  for (int n = 0; n < L; ++n)
+    for (int k = 0; k < L; ++k) {
+      const double v = inverse ? c[(size_t)k * L + n] : c[(size_t)n * L + k];
+      const int nb = n / 64, nl = n % 64, kc = k / kc_len, kk = k % kc_len;
+      uint8_t* slice = &img[(size_t)nb * PL::kBBytes];
+      if (FORM == tc::BF16X3) {
+        const float h = bf16_round(v);
+        const double r1 = v - h;
+        const float m = bf16_round(r1);
+        const float l = bf16_round(r1 - m);
+        const float parts[3] = {h, m, l};
+        const uint32_t off = tc::sw128(nl, kk / 8) + (kk % 8) * 2;
+        for (int sp = 0; sp < 3; ++sp) {
+          const uint16_t bits = bf16_bits(parts[sp]);
+          memcpy(slice + (size_t)(kc * 3 + sp) * tc::kBAtom + off, &bits, 2);
+        }
+      } else {
+        const float h = tf32_round(v);
+        const float l = tf32_round(v - h);
+        const float parts[2] = {h, l};
+        const uint32_t off = tc::sw128(nl, kk / 4) + (kk % 4) * 4;
+        for (int sp = 0; sp < 2; ++sp)
+          memcpy(slice + (size_t)(kc * 2 + sp) * tc::kBAtom + off, &parts[sp], 4);
+      }
+    }
+  return img;
+}
 
 std::mutex g_tc_mutex;
 std::map<int, TcDevice> g_tc;
@@ -148,6 +202,118 @@ bool make_map(CUtensorMap* m, const float* ptr, size_t rows) {
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(ptr), dims, strides, box, estr,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Row matrix (rows x L FP32) viewed by TMA in boxes of 32 x 128, 128-byte swizzle.
+bool make_rows_map(CUtensorMap* m, const float* ptr, size_t rows, int L) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)L, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)L * sizeof(float)};
+  cuuint32_t box[2] = {32, tc::kRows};
+  cuuint32_t estr[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(ptr), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int FORM, int L>
+const uint4* pass_image_device(TcDevice* d, bool inverse) {
+  constexpr int li = L == 64 ? 0 : L == 128 ? 1 : 2;
+  std::lock_guard<std::mutex> lock(g_tc_mutex);
+  void*& slot = d->pass_images[FORM][li][inverse ? 1 : 0];
+  if (!slot) {
+    const std::vector<uint8_t> img = pass_image<FORM, L>(inverse);
+    void* ptr = nullptr;
+    if (cudaMalloc(&ptr, img.size()) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(ptr, img.data(), img.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaFree(ptr);
+      return nullptr;
+    }
+    slot = ptr;
+  }
+  return reinterpret_cast<const uint4*>(slot);
+}
+
+// One row pass: rows x L matrix at x -> transposed arrays (R = 1 << rshift rows each) at out.
+template <int FORM, int L>
+int launch_pass(const bridct_plan* p, bool inverse, const float* x, float* out, size_t rows, int rshift,
+                cudaStream_t st, TcDevice* d) {
+  using PL = tc::PassLayout<FORM, L>;
+  auto k = tc::k_tcpass<FORM, L>;
+  static const bool attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                PL::kDynamic) == cudaSuccess;
+  if (!attr) return cuda_fail(cudaErrorInvalidConfiguration, "k_tcpass shared memory");
+  const uint4* img = pass_image_device<FORM, L>(d, inverse);
+  if (!img) return cuda_fail(cudaGetLastError(), "tensor-core coefficient upload");
+  CUtensorMap xm;
+  if (!make_rows_map(&xm, x, rows, L)) {
+    set_error("cuTensorMapEncodeTiled failed");
+    return BRIDCT_DEVICE_ERROR;
+  }
+  const long long mtiles = (long long)((rows + tc::kRows - 1) / tc::kRows);
+  long long slots = p->dev->sm_count / PL::kBlocks;
+  if (slots > mtiles) slots = mtiles;
+  if (slots < 1) slots = 1;
+  k<<<(unsigned)(slots * PL::kBlocks), tc::kWsThreads, PL::kDynamic, st>>>(xm, out, img, (long long)rows, rshift,
+                                                                         d->err);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_tcpass launch");
+}
+
+template <int FORM>
+int pass_by_length(const bridct_plan* p, int L, bool inverse, const float* x, float* out, size_t rows, int rshift,
+                   cudaStream_t st, TcDevice* d) {
+  switch (L) {
+    case 64: return launch_pass<FORM, 64>(p, inverse, x, out, rows, rshift, st, d);
+    case 128: return launch_pass<FORM, 128>(p, inverse, x, out, rows, rshift, st, d);
+    case 256: return launch_pass<FORM, 256>(p, inverse, x, out, rows, rshift, st, d);
+    default: return BRIDCT_INVALID_ARGUMENT;
+  }
+}
+
+int log2i(int v) {
+  int r = 0;
+  while ((1 << r) < v) ++r;
+  return r;
+}
+
+constexpr size_t kSepChunkBytes = size_t(48) << 20;   // arrays per pass pair: about 48 MB
+
+// Separable form: per batch of arrays, pass 1 (rows of W) x -> scratch, pass 2 (rows of H)
+// scratch -> y; the round trip runs the forward pair then the inverse pair on the same batch.
+template <int FORM>
+int apply_sep(bridct_plan* p, int mode, const float* x, float* y, size_t batch, cudaStream_t st, TcDevice* d) {
+  const size_t elems = (size_t)p->h * p->w;
+  size_t chunk = kSepChunkBytes / (elems * sizeof(float));
+  if (chunk < 1) chunk = 1;
+  if (chunk > batch) chunk = batch;
+  const size_t need = chunk * elems * sizeof(float);
+  if (p->tc_bytes < need) {
+    if (p->tc_mem) cudaFree(p->tc_mem);
+    p->tc_mem = nullptr;
+    p->tc_bytes = 0;
+    cudaError_t e = cudaMalloc(&p->tc_mem, need);
+    if (e != cudaSuccess) return cuda_fail(e, "tensor-core scratch");
+    p->tc_bytes = need;
+  }
+  float* t = static_cast<float*>(p->tc_mem);
+  const int lh = log2i(p->h), lw = log2i(p->w);
+  for (size_t b0 = 0; b0 < batch; b0 += chunk) {
+    const size_t nb = batch - b0 < chunk ? batch - b0 : chunk;
+    const float* xc = x + b0 * elems;
+    float* yc = y + b0 * elems;
+    for (int dir = 0; dir < 2; ++dir) {
+      const bool inverse = mode == 1 || dir == 1;
+      if (dir == 1 && mode != 2) break;
+      const float* src = dir == 0 ? xc : yc;
+      int s = pass_by_length<FORM>(p, p->w, inverse, src, t, nb * p->h, lh, st, d);
+      if (s) return s;
+      s = pass_by_length<FORM>(p, p->h, inverse, t, yc, nb * p->w, lw, st, d);
+      if (s) return s;
+    }
+  }
+  return BRIDCT_OK;
 }
 
 template <int FORM>
@@ -184,18 +350,25 @@ int apply_tc_form(bridct_plan* p, int mode, int form, const float* x, float* y, 
     set_error("unsupported execution form");
     return BRIDCT_INVALID_ARGUMENT;
   }
-  if (p->h != 8 || p->w != 8) {
-    set_error("the tensor-core forms cover batches of 8x8 arrays");
+  const bool sep_axis_h = p->h == 64 || p->h == 128 || p->h == 256;
+  const bool sep_axis_w = p->w == 64 || p->w == 128 || p->w == 256;
+  const bool kron = p->h == 8 && p->w == 8;
+  if (!kron && !(sep_axis_h && sep_axis_w)) {
+    set_error("the tensor-core forms cover 8x8 arrays and arrays whose axes are 64, 128 or 256");
     return BRIDCT_INVALID_ARGUMENT;
   }
-  const size_t bytes = batch * 64 * sizeof(float);
+  const size_t elems = (size_t)p->h * p->w;
+  const size_t bytes = batch * elems * sizeof(float);
   const uintptr_t a = (uintptr_t)x, b = (uintptr_t)y;
   if ((a <= b ? b - a : a - b) < bytes) return BRIDCT_OVERLAPPING_BUFFERS;
   if ((a | b) % 16) return BRIDCT_BAD_ALIGNMENT;
-  if (batch > (size_t)0x7FFFFFFF * tc::kRows) return BRIDCT_INVALID_ARGUMENT;
+  if (batch > (size_t)0x7FFFFFFF * tc::kRows / (elems / 64)) return BRIDCT_INVALID_ARGUMENT;
   TcDevice* d = tc_device(p->device);
   if (!d) return cuda_fail(cudaGetLastError(), "tensor-core setup");
   cudaStream_t st = (cudaStream_t)stream;
+  if (!kron)
+    return form == BRIDCT_FORM_TC_BF16X3 ? apply_sep<tc::BF16X3>(p, mode, x, y, batch, st, d)
+                                        : apply_sep<tc::TF32X3>(p, mode, x, y, batch, st, d);
   int s;
   if (mode == 2) {   // normalized round trip: forward into y, then inverse in place
     s = form == BRIDCT_FORM_TC_BF16X3 ? launch_tc8<tc::BF16X3>(p, 0, x, y, batch, st, d)

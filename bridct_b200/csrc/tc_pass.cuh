@@ -1,0 +1,336 @@
+// Tensor-core precision forms for arrays with axes of 64, 128 or 256 (tcgen05 + TMEM + TMA).
+//
+// A 2D transform Y = C_H X C_W^T is computed as two row passes.  A row pass takes a matrix of
+// contiguous rows of length L (rows grouped into arrays of R rows), multiplies every row by
+// C_L^T (forward) or C_L (inverse) on the tensor cores, and writes every array's result
+// transposed:
+//     pass 1: rows of X (R = H, L = W)      -> T_b = (X_b C_W^T)^T   (W x H per array)
+//     pass 2: rows of T (R = W, L = H)      -> Y_b = (T_b C_H^T)^T = C_H X_b C_W^T
+// so the second pass is again a plain row pass.  The host runs the passes over batches of
+// arrays small enough that T stays in L2 between them.
+//
+// One pass is a GEMM with M = rows (tiles of 128), N = L, K = L.  Each CTA owns one N-block of
+// 64 output columns: its slice of C_L (64 x L, split into bf16 or tf32 parts, in the K-major
+// 128-byte-swizzled image the UMMA B operand reads) is loaded into shared memory once, and the
+// CTA streams M-tiles through a TMA ring in K-chunks (64 FP32 per row for BF16x3, 32 for TF32x3).
+// Split precision as in the 8x8 forms: BF16x3 = six products of 3-way splits, TF32x3 = three
+// products of 2-way splits, all accumulated in FP32 in TMEM.
+//
+// Warp roles (384 threads):
+//   warp 0 lane 0  TMA producer: ring stage s <- K-chunk of an M-tile (waits stage_free)
+//   warp 1 lane 0  MMA issuer: TMEM acc set t += splits(stage s, A buffer a) . B slice; commits
+//                  stage_free/a_free per chunk and acc_full after an M-tile's last chunk
+//   warp 2         TMEM allocator
+//   warps 4-7      split: stage s (FP32) -> hi/mid in place + lo into A buffer a
+//   warps 8-11     epilogue: sum of acc set t -> registers (frees set t) -> transposed stores
+// Every wait is bounded; on expiry the CTA sets *err and all roles leave their loops.
+#pragma once
+#include "tc_blocks8.cuh"
+
+namespace bridct {
+namespace tc {
+
+template <int FORM> struct PassForm;
+template <> struct PassForm<BF16X3> {
+  static constexpr int kKC = 64;                         // FP32 row elements per K-chunk
+  static constexpr int kSplits = 3;
+  static constexpr int kStageBytes = kRows * kKC * 4;    // 32 KB (two 32-wide boxes)
+  static constexpr int kABufBytes = kRows * kKC * 2;     // Xl (bf16)
+};
+template <> struct PassForm<TF32X3> {
+  static constexpr int kKC = 32;
+  static constexpr int kSplits = 2;
+  static constexpr int kStageBytes = kRows * kKC * 4;    // 16 KB (one box)
+  static constexpr int kABufBytes = kRows * kKC * 4;     // Xl (tf32)
+};
+
+constexpr int kBAtom = 64 * 128;         // one K-major SW128 atom column of 64 B rows
+constexpr int kPassNBlock = 64;          // output columns per CTA (MMA N)
+constexpr int kPassSmemMax = 232448;     // opt-in shared memory per block
+constexpr int kPassMaxStages = 6;
+
+constexpr int pass_min(int a, int b) { return a < b ? a : b; }
+
+template <int FORM, int L>
+struct PassLayout {
+  using F = PassForm<FORM>;
+  static constexpr int kChunks = L / F::kKC;
+  static constexpr int kBlocks = L / kPassNBlock;
+  static constexpr int kBBytes = F::kSplits * kChunks * kBAtom;   // this CTA's slice of C_L
+  static constexpr int kABufs = 2;
+  static constexpr int kBarBytes = 1024;
+  static constexpr int kFixed = kBBytes + kABufs * F::kABufBytes + kBarBytes + 1024;
+  static constexpr int kStages = pass_min(kPassMaxStages, (kPassSmemMax - kFixed) / F::kStageBytes);
+  static_assert(kStages >= 2, "pass ring needs two stages");
+  static constexpr int kAOff = kStages * F::kStageBytes;
+  static constexpr int kBOff = kAOff + kABufs * F::kABufBytes;
+  static constexpr int kBarOff = kBOff + kBBytes;
+  static constexpr int kDynamic = kBarOff + kBarBytes + 1024;      // + 1024-byte alignment slack
+  static_assert(kDynamic <= kPassSmemMax, "shared memory budget");
+};
+
+struct PassBars {
+  uint32_t stage_full, stage_free, a_full, a_free, acc_full, acc_free, tmem_slot;
+  __device__ explicit PassBars(uint32_t b)
+      : stage_full(b), stage_free(b + 8 * kPassMaxStages), a_full(b + 16 * kPassMaxStages),
+        a_free(b + 16 * kPassMaxStages + 16), acc_full(b + 16 * kPassMaxStages + 32),
+        acc_free(b + 16 * kPassMaxStages + 48), tmem_slot(b + 16 * kPassMaxStages + 64) {}
+};
+
+// TF32 split of a one-box stage (128 rows x 32 FP32): Xh in place, Xl into the A buffer.
+__device__ __forceinline__ void split_box_tf32(uint8_t* stage, uint8_t* abuf, uint32_t r) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const uint32_t off = sw128(r, j);
+    uint4 h, l;
+    split_tf32x2(*reinterpret_cast<const float4*>(stage + off), h, l);
+    *reinterpret_cast<uint4*>(stage + off) = h;
+    *reinterpret_cast<uint4*>(abuf + off) = l;
+  }
+}
+
+// Accumulator set of one M-tile (64 TMEM columns per block).  The FP32 accumulation of an MMA
+// into a large accumulator loses the addends' low bits toward zero, so the dominant Xh.Ch
+// product accumulates apart from the small products (whose own losses are then negligible),
+// and over long K it is spread over kBig group accumulators by K-chunk, each receiving few
+// MMAs.  Products sharing an A split go into one MMA with the B splits stacked along N:
+//   BF16x3 blocks [big0 | small | smaller | big1]:
+//     Xh.[Ch|Cm|Cl] -> [big0|small|smaller] (group 0) or Xh.Ch -> big1, Xh.[Cm|Cl] -> [small|smaller]
+//     Xm.[Ch|Cm] -> [small|smaller],  Xl.Ch -> small
+//   TF32x3 blocks [big0 | small | big1 | big2]:
+//     Xh.[Ch|Cl] -> [big0|small] (group 0) or Xh.Ch -> big_g, Xh.Cl -> small;  Xl.Ch -> small
+// The epilogue adds the blocks in FP32.
+template <int FORM, int CHUNKS>
+struct PassAccs {
+  static constexpr int kMaxBig = FORM == BF16X3 ? 2 : 3;
+  static constexpr int kBig = CHUNKS < kMaxBig ? CHUNKS : kMaxBig;
+  static constexpr int kSmallBlocks = FORM == BF16X3 ? 2 : 1;
+  static constexpr int kPerTile = (1 + kSmallBlocks + (kBig - 1)) * kPassNBlock;   // columns
+  static constexpr int kExtraBig = (1 + kSmallBlocks) * kPassNBlock;               // big1 column
+  static constexpr int kAlloc = 2 * kPerTile <= 256 ? 256 : 512;
+  static_assert(2 * kPerTile <= 512, "TMEM columns");
+  __host__ __device__ static constexpr int group(int kc) { return kc * kBig / CHUNKS; }
+};
+
+// Split products of K-chunk kc (one thread).  sB: shared address of the B slice, laid out as
+// [chunk][split][8 KB atom column of 64 rows].  tmem: column 0 of this M-tile's set.
+template <int FORM, int CHUNKS>
+__device__ __forceinline__ void issue_pass_mmas(uint32_t sstage, uint32_t sabuf, uint32_t sB, int kc,
+                                                uint32_t tmem) {
+  using A = PassAccs<FORM, CHUNKS>;
+  const int g = A::group(kc);
+  const bool big_first = kc == 0 || A::group(kc - 1) != g;
+  const uint32_t big_g = tmem + A::kExtraBig + (uint32_t)(g - 1) * kPassNBlock;
+  const uint32_t bchunk = sB + (uint32_t)(kc * PassForm<FORM>::kSplits) * kBAtom;
+  if constexpr (FORM == BF16X3) {
+    constexpr uint32_t i192 = instr_desc(1, 192), i128 = instr_desc(1, 128), i64 = instr_desc(1, 64);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {   // 16 bf16 (32 bytes) per MMA
+      const uint64_t bd = sw128_desc(bchunk + k * 32u);
+      const uint64_t ah = sw128_desc(sstage + k * 32u);
+      if (g == 0) {
+        umma(tmem, ah, bd, i192, (kc | k) ? 1u : 0u, BF16X3);
+      } else {
+        umma(big_g, ah, bd, i64, (big_first && k == 0) ? 0u : 1u, BF16X3);
+        umma(tmem + 64, ah, sw128_desc(bchunk + kBAtom + k * 32u), i128, 1u, BF16X3);
+      }
+      umma(tmem + 64, sw128_desc(sstage + 16384u + k * 32u), bd, i128, 1u, BF16X3);   // Xm
+      umma(tmem + 64, sw128_desc(sabuf + k * 32u), bd, i64, 1u, BF16X3);              // Xl
+    }
+  } else {
+    constexpr uint32_t i128 = instr_desc(2, 128), i64 = instr_desc(2, 64);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {   // 8 tf32 (32 bytes) per MMA
+      const uint64_t bd = sw128_desc(bchunk + k * 32u);
+      const uint64_t ah = sw128_desc(sstage + k * 32u);
+      if (g == 0) {
+        umma(tmem, ah, bd, i128, (kc | k) ? 1u : 0u, TF32X3);
+      } else {
+        umma(big_g, ah, bd, i64, (big_first && k == 0) ? 0u : 1u, TF32X3);
+        umma(tmem + 64, ah, sw128_desc(bchunk + kBAtom + k * 32u), i64, 1u, TF32X3);
+      }
+      umma(tmem + 64, sw128_desc(sabuf + k * 32u), bd, i64, 1u, TF32X3);   // Xl
+    }
+  }
+}
+
+// xmap: the (nrows x L) FP32 row matrix (box 32 x 128, SWIZZLE_128B).  out: destination of
+// the transposed arrays (R rows per array, rshift = log2 R).  bimage: kBlocks slices of
+// PassLayout::kBBytes.  Grid: a multiple of kBlocks CTAs; CTA c computes N-block c % kBlocks.
+template <int FORM, int L>
+__global__ void __launch_bounds__(kWsThreads, 1)
+    k_tcpass(const __grid_constant__ CUtensorMap xmap, float* __restrict__ out,
+             const uint4* __restrict__ bimage, long long nrows, int rshift, int* __restrict__ err) {
+  using PL = PassLayout<FORM, L>;
+  using F = PassForm<FORM>;
+  constexpr int kStages = PL::kStages;
+  constexpr int kChunks = PL::kChunks;
+  using ACC = PassAccs<FORM, kChunks>;
+  constexpr uint32_t kTileCols = ACC::kPerTile;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t sbase = smem_u32(base);
+  const PassBars bars(sbase + PL::kBarOff);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + PL::kBarOff + 16 * kPassMaxStages + 64);
+  __shared__ volatile int s_abort;
+  __shared__ volatile int s_group_ok[2];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  const int nblk = blockIdx.x % PL::kBlocks;
+  const long long slot = blockIdx.x / PL::kBlocks;
+  const long long nslots = gridDim.x / PL::kBlocks;
+  const long long mtiles = (nrows + kRows - 1) / kRows;
+  const long long ntile_local = slot < mtiles ? (mtiles - 1 - slot) / nslots + 1 : 0;
+  const long long nchunk_local = ntile_local * kChunks;
+
+  if (tid == 0) {
+    s_abort = 0;
+    for (int i = 0; i < kStages; ++i) {
+      mbar_init(bars.stage_full + 8 * i, 1);
+      mbar_init(bars.stage_free + 8 * i, 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(bars.a_full + 8 * i, 1);
+      mbar_init(bars.a_free + 8 * i, 1);
+      mbar_init(bars.acc_full + 8 * i, 1);
+      mbar_init(bars.acc_free + 8 * i, 1);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(ACC::kAlloc));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  {
+    const uint4* src = bimage + (size_t)nblk * (PL::kBBytes / 16);
+    uint4* dst = reinterpret_cast<uint4*>(base + PL::kBOff);
+    for (int i = tid; i < PL::kBBytes / 16; i += kWsThreads) dst[i] = __ldg(src + i);
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  bool ok = true;
+
+  if (warp == 0 && lane == 0) {
+    for (long long j = 0; j < nchunk_local && ok && !s_abort; ++j) {
+      const int s = (int)(j % kStages);
+      ok = mbar_wait(bars.stage_free + 8 * s, ((uint32_t)(j / kStages) & 1u) ^ 1u);
+      if (!ok) break;
+      const long long m = slot + (j / kChunks) * nslots;
+      const int kc = (int)(j % kChunks);
+      const uint32_t dst = sbase + s * F::kStageBytes;
+      mbar_expect_tx(bars.stage_full + 8 * s, F::kStageBytes);
+      tma_load_2d(dst, &xmap, kc * F::kKC, (int)(m * kRows), bars.stage_full + 8 * s);
+      if constexpr (F::kKC == 64)
+        tma_load_2d(dst + 16384u, &xmap, kc * F::kKC + 32, (int)(m * kRows), bars.stage_full + 8 * s);
+    }
+  } else if (warp == 1 && lane == 0) {
+    for (long long j = 0; j < nchunk_local && ok && !s_abort; ++j) {
+      const int s = (int)(j % kStages), a = (int)(j & 1);
+      const long long jt = j / kChunks;
+      const int kc = (int)(j % kChunks), t = (int)(jt & 1);
+      ok = mbar_wait(bars.a_full + 8 * a, (uint32_t)(j >> 1) & 1u);
+      if (ok && kc == 0) ok = mbar_wait(bars.acc_free + 8 * t, ((uint32_t)(jt >> 1) & 1u) ^ 1u);
+      if (!ok) break;
+      tc_fence_after();
+      issue_pass_mmas<FORM, kChunks>(sbase + s * F::kStageBytes, sbase + PL::kAOff + a * F::kABufBytes,
+                                     sbase + PL::kBOff, kc, tmem_base + t * kTileCols);
+      umma_commit(bars.stage_free + 8 * s);
+      umma_commit(bars.a_free + 8 * a);
+      if (kc == kChunks - 1) umma_commit(bars.acc_full + 8 * t);
+    }
+    if (ok && nchunk_local > 0) {   // the last MMAs must finish before TMEM is freed
+      const long long j = nchunk_local - 1;
+      ok = mbar_wait(bars.a_free + 8 * (int)(j & 1), (uint32_t)(j >> 1) & 1u);
+    }
+  } else if (warp >= 4 && warp < 8) {
+    const uint32_t r = tid - 128;
+    for (long long j = 0; j < nchunk_local; ++j) {
+      const int s = (int)(j % kStages), a = (int)(j & 1);
+      if (r == 0) {
+        bool g = !s_abort && mbar_wait(bars.stage_full + 8 * s, (uint32_t)(j / kStages) & 1u);
+        if (g) g = mbar_wait(bars.a_free + 8 * a, ((uint32_t)(j >> 1) & 1u) ^ 1u);
+        s_group_ok[0] = g ? 1 : 0;
+      }
+      named_sync(1, 128);
+      if (!s_group_ok[0]) {
+        ok = r != 0;
+        break;
+      }
+      uint8_t* stage = base + s * F::kStageBytes;
+      uint8_t* abuf = base + PL::kAOff + a * F::kABufBytes;
+      if constexpr (FORM == BF16X3) split_tile<BF16X3>(stage, abuf, r);
+      else split_box_tf32(stage, abuf, r);
+      fence_async_smem();
+      named_sync(1, 128);
+      if (r == 0) mbar_arrive(bars.a_full + 8 * a);
+    }
+  } else if (warp >= 8) {
+    const uint32_t r = tid - 256;                 // tile row = TMEM lane
+    const uint32_t quarter = (uint32_t)(warp & 3) * 32u;
+    const long long rmask = (1ll << rshift) - 1;
+    for (long long jt = 0; jt < ntile_local; ++jt) {
+      const int t = (int)(jt & 1);
+      if (r == 0)
+        s_group_ok[1] = (!s_abort && mbar_wait(bars.acc_full + 8 * t, (uint32_t)(jt >> 1) & 1u)) ? 1 : 0;
+      named_sync(2, 128);
+      if (!s_group_ok[1]) {
+        ok = r != 0;
+        break;
+      }
+      tc_fence_after();
+      float v[kPassNBlock];
+      const uint32_t taddr = tmem_base + t * kTileCols + (quarter << 16);
+#pragma unroll
+      for (int q = 0; q < kPassNBlock / 16; ++q) {
+        float big[16], sm[16], w[16];
+        tmem_ld16(taddr + q * 16, big);
+        tmem_ld16(taddr + kPassNBlock + q * 16, sm);
+        tmem_wait_ld();
+#pragma unroll
+        for (int a = 0; a < ACC::kSmallBlocks - 1; ++a) {
+          tmem_ld16(taddr + (2 + a) * kPassNBlock + q * 16, w);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) sm[i] += w[i];
+        }
+#pragma unroll
+        for (int a = 1; a < ACC::kBig; ++a) {
+          tmem_ld16(taddr + ACC::kExtraBig + (a - 1) * kPassNBlock + q * 16, w);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) big[i] += w[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[q * 16 + i] = big[i] + sm[i];
+      }
+      tc_fence_before();
+      named_sync(2, 128);
+      if (r == 0) mbar_arrive(bars.acc_free + 8 * t);
+      // row g = (array b, row h of that array); its column n goes to out[b][n][h]
+      const long long g = (slot + jt * nslots) * kRows + r;
+      if (g < nrows) {
+        const long long b = g >> rshift, h = g & rmask;
+        float* dst = out + ((b * L + (long long)nblk * kPassNBlock) << rshift) + h;
+#pragma unroll
+        for (int c = 0; c < kPassNBlock; ++c) dst[(long long)c << rshift] = v[c];
+      }
+    }
+  }
+  if (!ok) {
+    s_abort = 1;
+    atomicExch(err, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 2) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(ACC::kAlloc));
+  }
+}
+
+}  // namespace tc
+}  // namespace bridct
