@@ -138,6 +138,14 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       : "memory");
 }
 
+// Brings a box of the tensor into L2 ahead of its load (no shared memory, no completion).
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y)
+               : "memory");
+}
+
 __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int y, uint32_t src) {
   asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
                    reinterpret_cast<uint64_t>(map)),
@@ -253,25 +261,41 @@ __device__ __forceinline__ void split_tile(uint8_t* stage, uint8_t* abuf, uint32
         *reinterpret_cast<uint4*>(abuf + off) = l;
       }
   } else {
-    // Row r's 64 FP32 values (box 0 row r: elements 0..31, box 1 row r: 32..63) are read
-    // first; bf16 chunk j' (elements 8j'..8j'+7) of Xh then goes to box 0 row r, of Xm to box 1
-    // row r, of Xl to the A buffer, all in the K-major SW128 layout.
-    float x[64];
+    // Row r holds 64 FP32 values: box 0 row r = elements 0..31, box 1 row r = 32..63.  bf16
+    // chunk jp (elements 8jp..8jp+7) of Xh goes to box 0 row r chunk jp, of Xm to box 1 row r
+    // chunk jp, of Xl to the A buffer, all in the K-major SW128 layout.  Box 0 is split first;
+    // its Xm chunks would overwrite box 1 values not yet read, so they are held in registers
+    // until box 1 has been read and split.
+    uint32_t mid0[4][4];
 #pragma unroll
-    for (int c = 0; c < 16; ++c) {
-      const float4 u = *reinterpret_cast<const float4*>(stage + (c >> 3) * 16384u + sw128(r, c & 7));
-      x[4 * c] = u.x; x[4 * c + 1] = u.y; x[4 * c + 2] = u.z; x[4 * c + 3] = u.w;
+    for (int half = 0; half < 2; ++half) {
+      float x[32];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const float4 u = *reinterpret_cast<const float4*>(stage + half * 16384u + sw128(r, c));
+        x[4 * c] = u.x; x[4 * c + 1] = u.y; x[4 * c + 2] = u.z; x[4 * c + 3] = u.w;
+      }
+#pragma unroll
+      for (int jq = 0; jq < 4; ++jq) {
+        const int jp = half * 4 + jq;
+        uint32_t hi[4], mid[4], lo[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) split_bf16x3_pair(x[8 * jq + 2 * e], x[8 * jq + 2 * e + 1], hi[e], mid[e], lo[e]);
+        const uint32_t off = sw128(r, jp);
+        *reinterpret_cast<uint4*>(stage + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4*>(abuf + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        if (half == 1) {
+          *reinterpret_cast<uint4*>(stage + 16384u + off) = make_uint4(mid[0], mid[1], mid[2], mid[3]);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) mid0[jq][e] = mid[e];
+        }
+      }
     }
 #pragma unroll
-    for (int jp = 0; jp < 8; ++jp) {
-      uint32_t hi[4], mid[4], lo[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) split_bf16x3_pair(x[8 * jp + 2 * e], x[8 * jp + 2 * e + 1], hi[e], mid[e], lo[e]);
-      const uint32_t off = sw128(r, jp);
-      *reinterpret_cast<uint4*>(stage + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-      *reinterpret_cast<uint4*>(stage + 16384u + off) = make_uint4(mid[0], mid[1], mid[2], mid[3]);
-      *reinterpret_cast<uint4*>(abuf + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-    }
+    for (int jq = 0; jq < 4; ++jq)
+      *reinterpret_cast<uint4*>(stage + 16384u + sw128(r, jq)) =
+          make_uint4(mid0[jq][0], mid0[jq][1], mid0[jq][2], mid0[jq][3]);
   }
 }
 

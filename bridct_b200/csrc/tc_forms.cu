@@ -8,7 +8,8 @@
 //
 // Axes of 64, 128 and 256 (any combination): two row passes of k_tcpass per batch of arrays
 // (pass 1 over rows of length W into a plan-owned scratch, pass 2 over rows of length H into
-// the output), with the batch cut so that the scratch stays in L2 between the passes.  The B
+// the output), with the batch cut so that the scratch stays in L2 between the passes; BF16x3 on
+// 64x64 arrays runs both passes in one launch (k_tc64) with the intermediate on chip.  The B
 // images hold C_L (or C_L^T for the inverse) split into bf16 or tf32 parts, one 64-row slice
 // per N-block, in the K-major 128-byte-swizzled layout.
 #include <cuda.h>
@@ -25,6 +26,7 @@
 #include "bridct_internal.h"
 #include "tc_blocks8.cuh"
 #include "tc_pass.cuh"
+#include "tc_fused64.cuh"
 
 namespace bridct {
 namespace {
@@ -261,6 +263,27 @@ int launch_pass(const bridct_plan* p, bool inverse, const float* x, float* out, 
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_tcpass launch");
 }
 
+// BF16x3 on 64x64 arrays: both passes in one launch of k_tc64.
+int launch_fused64(const bridct_plan* p, bool inverse, const float* x, float* y, size_t batch, cudaStream_t st,
+                   TcDevice* d) {
+  using F = tc::Fused64;
+  static const bool attr =
+      cudaFuncSetAttribute(tc::k_tc64, cudaFuncAttributeMaxDynamicSharedMemorySize, F::kDynamic) == cudaSuccess;
+  if (!attr) return cuda_fail(cudaErrorInvalidConfiguration, "k_tc64 shared memory");
+  const uint4* img = pass_image_device<tc::BF16X3, 64>(d, inverse);
+  if (!img) return cuda_fail(cudaGetLastError(), "tensor-core coefficient upload");
+  CUtensorMap xm;
+  if (!make_rows_map(&xm, x, batch * 64, 64)) {
+    set_error("cuTensorMapEncodeTiled failed");
+    return BRIDCT_DEVICE_ERROR;
+  }
+  const long long tiles = (long long)((batch + 1) / 2);
+  const long long grid = tiles < p->dev->sm_count ? tiles : p->dev->sm_count;
+  tc::k_tc64<<<(unsigned)grid, F::kThreads, F::kDynamic, st>>>(xm, y, img, (long long)batch, d->err);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_tc64 launch");
+}
+
 template <int FORM>
 int pass_by_length(const bridct_plan* p, int L, bool inverse, const float* x, float* out, size_t rows, int rshift,
                    cudaStream_t st, TcDevice* d) {
@@ -284,6 +307,11 @@ constexpr size_t kSepChunkBytes = size_t(48) << 20;   // arrays per pass pair: a
 // scratch -> y; the round trip runs the forward pair then the inverse pair on the same batch.
 template <int FORM>
 int apply_sep(bridct_plan* p, int mode, const float* x, float* y, size_t batch, cudaStream_t st, TcDevice* d) {
+  if (FORM == tc::BF16X3 && p->h == 64 && p->w == 64) {
+    int s = launch_fused64(p, mode == 1, x, y, batch, st, d);
+    if (s || mode != 2) return s;
+    return launch_fused64(p, true, y, y, batch, st, d);   // each CTA rewrites only tiles it has read
+  }
   const size_t elems = (size_t)p->h * p->w;
   size_t chunk = kSepChunkBytes / (elems * sizeof(float));
   if (chunk < 1) chunk = 1;
