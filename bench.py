@@ -78,7 +78,18 @@ def workload(name: str):
         rng = np.random.default_rng(4)
         mag = 10.0 ** rng.uniform(-6, 6, (2048, 256, 256))
         x = (mag * rng.choice([-1.0, 1.0], size=mag.shape)).astype(np.float32)
-        return dict(x=x, mode=0, desc="2048 arrays 256x256 log-uniform 1e-6..1e6 (seed 4), forward")
+        del mag
+        # 1% of the arrays (21, drawn by the same generator) become a unit impulse or a constant
+        special = sorted(int(i) for i in rng.choice(2048, 21, replace=False))
+        for i in special:
+            if rng.integers(0, 2):
+                x[i] = 0.0
+                x[i, rng.integers(0, 256), rng.integers(0, 256)] = 1.0
+            else:
+                x[i] = np.float32(rng.choice([-1.0, 1.0]) * 10.0 ** rng.uniform(-6, 6))
+        return dict(x=x, mode=0, check=special,
+                    desc="2048 arrays 256x256 log-uniform 1e-6..1e6 with random signs, 21 of "
+                    "them a unit impulse or a constant (seed 4), forward")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -262,7 +273,8 @@ def main():
     ap.add_argument("--workload", default="blocks8")
     ap.add_argument("--form", default="auto")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--batch", type=int, default=0, help="use only the first N arrays of the workload")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="use the first N arrays of the workload (repeated cyclically when N is larger)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -296,7 +308,7 @@ def main():
         return run_ragged(args, wl, rank, world, local, dist, torch)
     xh = wl["x"]
     if args.batch:
-        xh = np.ascontiguousarray(xh[:args.batch])
+        xh = np.ascontiguousarray(np.resize(xh, (args.batch,) + xh.shape[1:]))
     b, h, w = xh.shape
     mode = wl["mode"]
     bytes_step = 8.0 * b * h * w
@@ -322,7 +334,8 @@ def main():
                              "tc_fp8": _lib.FORM_TC_FP8}[args.form]}
 
     # accuracy of each form on a sample, against float64 (equal-error comparison)
-    sample = slice(0, min(b, 4096 if h * w <= 4096 else 8))
+    sample = list(range(min(b, 4096 if h * w <= 4096 else 8)))
+    sample += [i for i in wl.get("check", []) if i < b and i not in sample]
     xs_np = xh[sample]
     exact = O.fp64_apply(xs_np, mode)
     results = {}
