@@ -222,7 +222,7 @@ BRIDCT_API void bridct_plan_destroy(bridct_plan* plan) {
   cudaGetDevice(&prev);
   cudaSetDevice(plan->device);
   if (plan->stream) cudaStreamSynchronize(plan->stream);
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < 3; ++i)
     if (plan->aux[i]) {
       cudaStreamSynchronize(plan->aux[i]);
       cudaStreamDestroy(plan->aux[i]);

@@ -44,10 +44,13 @@ struct bridct_plan {
   float* d_x = nullptr;        // one-array device staging
   float* d_y = nullptr;
   float* pin = nullptr;        // one-array pinned staging (in, out)
-  // batch pipeline (allocated on the first host-pointer batch call)
-  cudaStream_t aux[2] = {nullptr, nullptr};
-  float* d_batch = nullptr;    // 2 slots x (in, out) x chunk
-  float* pin_batch = nullptr;  // 2 slots x (in, out) x chunk, pageable callers only
+  // batch pipeline (allocated on the first host-pointer batch call): copy-in, kernel and
+  // copy-out streams, and per slot the events that order a slot's reuse on the GPU
+  static constexpr int kPipeSlots = 4;
+  cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t pipe_ev[3][kPipeSlots] = {};   // [copied in, transformed, copied out][slot]
+  float* d_batch = nullptr;    // slots x (in, out) x chunk
+  float* pin_batch = nullptr;  // slots x (in, out) x chunk, pageable callers only
   size_t chunk = 0;            // arrays per pipeline chunk
   // precision-form scratch (allocated on first use of a tensor-core form)
   void* tc_mem = nullptr;

@@ -12,99 +12,136 @@
 
 namespace bridct {
 
-static constexpr size_t kChunkBytes = 16u << 20;   // per slot and direction
+static constexpr size_t kChunkBytes = 8u << 20;      // staging per slot and direction
+static constexpr size_t kMinChunkBytes = 4u << 20;   // smallest chunk a call cuts
+static constexpr int kSlots = bridct_plan::kPipeSlots;
 
 static int ensure_batch_staging(bridct_plan* p, bool need_pinned) {
   const size_t per = p->elements * sizeof(float);
   if (!p->d_batch) {
     size_t c = kChunkBytes / per;
     p->chunk = c ? c : 1;
-    cudaError_t e = cudaMalloc((void**)&p->d_batch, 4 * p->chunk * per);
+    cudaError_t e = cudaMalloc((void**)&p->d_batch, 2 * kSlots * p->chunk * per);
     if (e != cudaSuccess) return cuda_fail(e, "batch staging");
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < 3; ++i) {
       e = cudaStreamCreateWithFlags(&p->aux[i], cudaStreamNonBlocking);
       if (e != cudaSuccess) return cuda_fail(e, "batch streams");
+      for (int k = 0; k < kSlots; ++k) {
+        e = cudaEventCreateWithFlags(&p->pipe_ev[i][k], cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(e, "batch events");
+      }
     }
   }
   if (need_pinned && !p->pin_batch) {
-    cudaError_t e = cudaHostAlloc((void**)&p->pin_batch, 4 * p->chunk * per, cudaHostAllocDefault);
+    cudaError_t e = cudaHostAlloc((void**)&p->pin_batch, 2 * kSlots * p->chunk * per, cudaHostAllocDefault);
     if (e != cudaSuccess) return cuda_fail(e, "pinned batch staging");
   }
   return BRIDCT_OK;
 }
 
-// Chunks of the batch alternate between two slots, each with its own stream, so that the
-// copy engines (H2D, D2H) and the SMs work on different chunks at the same time.
+// Chunks of the batch rotate through kSlots staging slots.  Copies in run on one stream, the
+// transforms on a second and copies out on a third, so both copy engines and the SMs work on
+// different chunks at once; a slot's reuse is ordered on the GPU by its events (the next copy
+// in waits for the transform that read the slot, the next transform for the copy out that read
+// it).  The host waits only where it copies through its own pinned staging (pageable callers)
+// and at the end.
 int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, size_t batch,
                         const float* dx, float* dy, bool pin_in, bool pin_out) {
   const bool stage_in = !dx && !pin_in, stage_out = !dy && !pin_out;
   int s = ensure_batch_staging(p, stage_in || stage_out);
   if (s) return s;
   const size_t per = p->elements;              // floats per array
-  const size_t cf = p->chunk * per;            // floats per chunk
-  const size_t cbytes = cf * sizeof(float);
+  const size_t cf = p->chunk * per;            // floats per staging slot
+  // About eight chunks per call (the first copy in and the last copy out do not overlap the
+  // other direction), each between kMinChunkBytes and the slot size: PCIe copies below a
+  // few MB lose efficiency.
+  size_t chunk = (batch + 7) / 8;
+  const size_t min_chunk = kMinChunkBytes / (per * sizeof(float));
+  if (chunk < min_chunk) chunk = min_chunk;
+  if (chunk > p->chunk) chunk = p->chunk;
+  if (chunk < 1) chunk = 1;
   const bool dx_ok = dx && (uintptr_t)dx % 16 == 0, dy_ok = dy && (uintptr_t)dy % 16 == 0;
-  size_t pending_off[2] = {0, 0}, pending_n[2] = {0, 0};
-  bool pending[2] = {false, false};
+  cudaStream_t hs = p->aux[0], ks = p->aux[1], ds = p->aux[2];
+  cudaEvent_t* ev_in = p->pipe_ev[0];
+  cudaEvent_t* ev_k = p->pipe_ev[1];
+  cudaEvent_t* ev_out = p->pipe_ev[2];
+  size_t pending_off[kSlots] = {}, pending_n[kSlots] = {};
+  bool used[kSlots] = {}, pending[kSlots] = {};
   cudaError_t e = cudaSuccess;
   size_t ci = 0;
-  for (size_t a0 = 0; a0 < batch; a0 += p->chunk, ++ci) {
-    const int slot = (int)(ci & 1);
-    cudaStream_t st = p->aux[slot];
-    const size_t na = batch - a0 < p->chunk ? batch - a0 : p->chunk;
+  for (size_t a0 = 0; a0 < batch; a0 += chunk, ++ci) {
+    const int slot = (int)(ci % kSlots);
+    const size_t na = batch - a0 < chunk ? batch - a0 : chunk;
     const size_t off = a0 * per, nbytes = na * per * sizeof(float);
     float* sx = p->d_batch + (size_t)slot * 2 * cf;
     float* sy = sx + cf;
     float* px = p->pin_batch ? p->pin_batch + (size_t)slot * 2 * cf : nullptr;
     float* py = px ? px + cf : nullptr;
-    if (pending[slot]) {        // slot reuse: finish the chunk that used it before
-      e = cudaStreamSynchronize(st);
+    if (pending[slot]) {        // the host copies the slot's previous output out of pinned staging
+      e = cudaEventSynchronize(ev_out[slot]);
       if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");
-      if (stage_out) memcpy(out + pending_off[slot], py, pending_n[slot]);
+      memcpy(out + pending_off[slot], py, pending_n[slot]);
       pending[slot] = false;
     }
     const float* kx;
     if (dx_ok) {
       kx = dx + off;
     } else {
-      if (dx) {
-        e = cudaMemcpyAsync(sx, dx + off, nbytes, cudaMemcpyDeviceToDevice, st);
-      } else if (pin_in) {
-        e = cudaMemcpyAsync(sx, in + off, nbytes, cudaMemcpyHostToDevice, st);
-      } else {
-        memcpy(px, in + off, nbytes);
-        e = cudaMemcpyAsync(sx, px, nbytes, cudaMemcpyHostToDevice, st);
+      if (used[slot]) {
+        e = cudaStreamWaitEvent(hs, ev_k[slot], 0);   // the slot's last transform has read sx
+        if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");
       }
+      if (dx) {
+        e = cudaMemcpyAsync(sx, dx + off, nbytes, cudaMemcpyDeviceToDevice, hs);
+      } else if (pin_in) {
+        e = cudaMemcpyAsync(sx, in + off, nbytes, cudaMemcpyHostToDevice, hs);
+      } else {
+        if (used[slot]) {      // px is free once the slot's last copy in has read it
+          e = cudaEventSynchronize(ev_in[slot]);
+          if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");
+        }
+        memcpy(px, in + off, nbytes);
+        e = cudaMemcpyAsync(sx, px, nbytes, cudaMemcpyHostToDevice, hs);
+      }
+      if (e == cudaSuccess) e = cudaEventRecord(ev_in[slot], hs);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(ks, ev_in[slot], 0);
       if (e != cudaSuccess) return cuda_fail(e, "batch H2D");
       kx = sx;
     }
     float* ky = dy_ok ? dy + off : sy;
-    s = launch_plain_form(p, mode, kx, ky, (long long)na, st);
+    if (!dy_ok && used[slot]) {
+      e = cudaStreamWaitEvent(ks, ev_out[slot], 0);     // the slot's last copy out has read sy
+      if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");
+    }
+    s = launch_plain_form(p, mode, kx, ky, (long long)na, ks);
     if (s) return s;
+    e = cudaEventRecord(ev_k[slot], ks);
+    if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");
     if (!dy_ok) {
-      if (dy) {
-        e = cudaMemcpyAsync(dy + off, sy, nbytes, cudaMemcpyDeviceToDevice, st);
-      } else if (pin_out) {
-        e = cudaMemcpyAsync(out + off, sy, nbytes, cudaMemcpyDeviceToHost, st);
-      } else {
-        e = cudaMemcpyAsync(py, sy, nbytes, cudaMemcpyDeviceToHost, st);
-        pending_off[slot] = off;
-        pending_n[slot] = nbytes;
+      e = cudaStreamWaitEvent(ds, ev_k[slot], 0);
+      if (e == cudaSuccess) {
+        if (dy) {
+          e = cudaMemcpyAsync(dy + off, sy, nbytes, cudaMemcpyDeviceToDevice, ds);
+        } else if (pin_out) {
+          e = cudaMemcpyAsync(out + off, sy, nbytes, cudaMemcpyDeviceToHost, ds);
+        } else {
+          e = cudaMemcpyAsync(py, sy, nbytes, cudaMemcpyDeviceToHost, ds);
+          pending_off[slot] = off;
+          pending_n[slot] = nbytes;
+          pending[slot] = true;
+        }
       }
+      if (e == cudaSuccess) e = cudaEventRecord(ev_out[slot], ds);
       if (e != cudaSuccess) return cuda_fail(e, "batch D2H");
     }
-    pending[slot] = true;
-    (void)cbytes;
+    used[slot] = true;
   }
-  for (int slot = 0; slot < 2; ++slot) {
-    if (!pending[slot]) continue;
-    e = cudaStreamSynchronize(p->aux[slot]);
+  for (int i = 0; i < 3; ++i) {
+    e = cudaStreamSynchronize(p->aux[i]);
     if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");
-    if (stage_out) {
-      float* py = p->pin_batch + (size_t)slot * 2 * cf + cf;
-      memcpy(out + pending_off[slot], py, pending_n[slot]);
-    }
   }
+  for (int slot = 0; slot < kSlots; ++slot)
+    if (pending[slot]) memcpy(out + pending_off[slot], p->pin_batch + (size_t)slot * 2 * cf + cf, pending_n[slot]);
   return BRIDCT_OK;
 }
 
@@ -126,6 +163,12 @@ bridct_plan* thread_square_plan(int n) {
 void release_plan_extras(bridct_plan* p) {
   if (p->tc_mem) cudaFree(p->tc_mem);
   p->tc_mem = nullptr;
+  for (auto& row : p->pipe_ev)
+    for (cudaEvent_t& ev : row)
+      if (ev) {
+        cudaEventDestroy(ev);
+        ev = nullptr;
+      }
 }
 
 }  // namespace bridct
