@@ -273,6 +273,10 @@ def main():
     ap.add_argument("--workload", default="blocks8")
     ap.add_argument("--form", default="auto")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--autotune", action="store_true",
+                    help="ragged workload: measure the unit geometry first and record it (see --tuning-out)")
+    ap.add_argument("--tuning-out", default="", help="where --autotune writes its result "
+                    "(default profiles/ragged_tuning.json)")
     ap.add_argument("--batch", type=int, default=0,
                     help="use the first N arrays of the workload (repeated cyclically when N is larger)")
     args = ap.parse_args()
@@ -451,12 +455,20 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
     from oracle import oracle as O
 
     dev = torch.device("cuda", local)
+    x = torch.from_numpy(wl["x"]).to(dev)
     tuning = None
     tfile = ROOT / "profiles" / "ragged_tuning.json"
-    if tfile.exists():
+    if args.autotune:
+        from bridct_b200.autotune import tune
+
+        res = tune(wl["items"], x)
+        tuning = res["best"]
+        if rank == 0:
+            out_path = Path(args.tuning_out) if args.tuning_out else tfile
+            out_path.write_text(json.dumps({"workload": wl["desc"], **res}, indent=1) + "\n")
+    elif tfile.exists():
         tuning = json.loads(tfile.read_text()).get("best")
     batch = RaggedBatch(wl["items"], tuning=tuning)
-    x = torch.from_numpy(wl["x"]).to(dev)
     y = torch.empty_like(x)
     stream = torch.cuda.Stream(device=dev)
     bytes_step = 8.0 * batch.span

@@ -1,0 +1,95 @@
+"""Autotuner for the batching form: picks the work-unit geometry of a ragged batch.
+
+The persistent ragged kernel cuts a batch into units per shape class: whole arrays up to
+`tile_floats` (both passes in one unit), column strips of `strip_floats` and row blocks of
+`row_floats` for larger arrays, with `lookahead` larger arrays' strips queued ahead of their row
+passes.  The best geometry depends on the batch's mix of shapes, so it is measured:
+
+    from bridct_b200.autotune import tune
+    result = tune(items, x)            # items: [(h, w, mode)], x: packed float32 CUDA tensor
+    batch = RaggedBatch(items, tuning=result["best"])
+
+The search is coordinate descent from the library default over the candidate values below (two
+sweeps), each candidate timed with CUDA events around CUDA-graph replays of the persistent
+launch on the caller's data.  Every candidate result is checked against the default geometry's
+output before its time counts.
+"""
+from __future__ import annotations
+
+from typing import Dict, List, Optional, Sequence, Tuple
+
+CANDIDATES: Dict[str, Sequence[int]] = {
+    "tile_floats": (1024, 2048, 4096, 8192, 16384),
+    "strip_floats": (2048, 4096, 8192, 16384),
+    "row_floats": (2048, 4096, 8192, 16384),
+    "lookahead": (1, 2, 4, 8, 16),
+}
+
+
+def default_tuning() -> Dict[str, int]:
+    from . import _lib
+
+    t = _lib.RaggedTuning()
+    _lib.lib().bridct_ragged_default_tuning(t)
+    return {k: int(getattr(t, k)) for k in CANDIDATES}
+
+
+def time_tuning(items, x, tuning: Dict[str, int], steps: int = 8, reference=None) -> Tuple[float, object]:
+    """Milliseconds per persistent launch with `tuning` (graph replays); returns (ms, output)."""
+    import torch
+
+    from .ragged import RaggedBatch
+
+    batch = RaggedBatch(items, tuning=tuning)
+    y = torch.empty_like(x)
+    stream = torch.cuda.Stream(device=x.device)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            batch.apply(x, y, stream=stream.cuda_stream)
+    stream.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        for _ in range(steps):
+            batch.apply(x, y, stream=stream.cuda_stream)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        g.replay()                      # warm the graph
+        start.record(stream)
+        g.replay()
+        end.record(stream)
+    end.synchronize()
+    del g
+    if batch.timed_out():
+        raise RuntimeError(f"ragged launch reported a bounded-wait expiry with tuning {tuning}")
+    if reference is not None:
+        scale = float(reference.abs().max()) or 1.0
+        if float((y - reference).abs().max()) > 1e-5 * scale:
+            raise RuntimeError(f"ragged output with tuning {tuning} disagrees with the default geometry")
+    return start.elapsed_time(end) / steps, y
+
+
+def tune(items, x, candidates: Optional[Dict[str, Sequence[int]]] = None, sweeps: int = 2,
+         steps: int = 8) -> Dict[str, object]:
+    """Coordinate descent over `candidates`; returns {"best", "best_ms", "default_ms", "table"}."""
+    candidates = candidates or CANDIDATES
+    best = default_tuning()
+    base_ms, reference = time_tuning(items, x, best, steps)
+    table: List[Dict[str, object]] = [{"tuning": dict(best), "ms": base_ms}]
+    seen = {tuple(sorted(best.items())): base_ms}
+    best_ms = base_ms
+    for _ in range(sweeps):
+        improved = False
+        for key, values in candidates.items():
+            for v in values:
+                trial = dict(best, **{key: int(v)})
+                sig = tuple(sorted(trial.items()))
+                if sig in seen:
+                    continue
+                ms, _ = time_tuning(items, x, trial, steps, reference)
+                seen[sig] = ms
+                table.append({"tuning": trial, "ms": ms})
+                if ms < best_ms * 0.995:
+                    best, best_ms, improved = trial, ms, True
+        if not improved:
+            break
+    return {"best": best, "best_ms": best_ms, "default_ms": base_ms, "table": table}

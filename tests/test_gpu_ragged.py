@@ -55,7 +55,8 @@ def test_ragged_matches_launch_loop():
 
 
 @pytest.mark.parametrize("tuning", [dict(tile_floats=4096, strip_floats=4096, row_floats=4096, lookahead=1),
-                                    dict(tile_floats=16384, strip_floats=8192, row_floats=16384, lookahead=8)])
+                                    dict(tile_floats=16384, strip_floats=8192, row_floats=16384, lookahead=8),
+                                    dict(tile_floats=1024, strip_floats=2048, row_floats=2048, lookahead=16)])
 def test_ragged_tunings_agree(tuning):
     items = random_batch(60, 9)
     x = torch.randn(RaggedBatch(items).span, device="cuda")
@@ -95,3 +96,20 @@ def test_ragged_rejects_bad_items():
         RaggedBatch([(8, 8, 0), (8, 8, 0)], offsets=[0, 32])     # overlap
     with pytest.raises(ValueError):
         RaggedBatch([(8, 8, 0)], offsets=[2])                    # misaligned
+
+
+def test_autotune_picks_a_measured_geometry():
+    from bridct_b200.autotune import tune
+
+    items = random_batch(48, 5)
+    x = torch.randn(RaggedBatch(items).span, device="cuda")
+    cands = {"tile_floats": (4096, 16384), "lookahead": (1, 4)}
+    res = tune(items, x, candidates=cands, sweeps=1, steps=2)
+    assert res["best_ms"] <= res["default_ms"]
+    assert len(res["table"]) >= 3
+    assert all(k in res["best"] for k in ("tile_floats", "strip_floats", "row_floats", "lookahead"))
+    b = RaggedBatch(items)
+    ref = b.apply(x)
+    got = RaggedBatch(items, tuning=res["best"]).apply(x)
+    torch.cuda.synchronize()
+    close(ref, got, x, items, b)
