@@ -2,7 +2,7 @@
 tensor-core split-precision forms, with the reference's own CPU path timed on the host.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload blocks8|arrays64|large1024|ragged|sweep256] [--form auto|sj|...]
+                    [--workload blocks8|image8|arrays64|large1024|ragged|sweep256] [--form auto|sj|...]
 
 Default workload: 262,144 independent 8x8 blocks of a 4096x4096 image (pixels uniform integers
 0..255 minus 128, seed 1), forward DCT-II, blocks stored contiguously as (B, 8, 8).  A step is
@@ -56,6 +56,10 @@ def workload(name: str):
         x = img.reshape(512, 8, 512, 8).transpose(0, 2, 1, 3).reshape(-1, 8, 8).copy()
         return dict(x=x, mode=0, desc="262,144 independent 8x8 blocks of a 4096x4096 image "
                     "(U{0..255}-128, seed 1), forward DCT-II, contiguous (B,8,8)")
+    if name == "image8":
+        img = (np.random.default_rng(1).integers(0, 256, (4096, 4096)) - 128).astype(np.float32)
+        return dict(x=img, mode=0, desc="4096x4096 image (U{0..255}-128, seed 1): its 262,144 8x8 blocks "
+                    "transformed where they lie (block-strided reads and writes), forward DCT-II")
     if name == "arrays64":
         x = np.random.default_rng(0).uniform(-1, 1, (1024, 64, 64)).astype(np.float32)
         return dict(x=x, mode=0, desc="1024 arrays 64x64 U[-1,1] (seed 0), forward DCT-II")
@@ -310,6 +314,8 @@ def main():
     wl = workload(args.workload)
     if args.workload == "ragged":
         return run_ragged(args, wl, rank, world, local, dist, torch)
+    if args.workload == "image8":
+        return run_image8(args, wl, rank, world, local, dist, torch)
     xh = wl["x"]
     if args.batch:
         xh = np.ascontiguousarray(np.resize(xh, (args.batch,) + xh.shape[1:]))
@@ -523,6 +529,106 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
             "forms": out, "max_rel_err_output_scaled_sample": worst,
             "speedup_vs_launch_loop": out["launch_loop"]["ms_per_step"] / head["ms_per_step"],
             "clocks": head["clocks"], "gpu_launches": head["steps"]}))
+
+
+def run_image8(args, wl, rank, world, local, dist, torch):
+    """8x8 blocks read and written in place inside the image (block-strided), one launch per step."""
+    from bridct_b200 import torch_api
+    from bridct_b200.dist import max_over_ranks
+    from oracle import oracle as O
+
+    dev = torch.device("cuda", local)
+    img = wl["x"]
+    h, w = img.shape
+    steps_q = np.fromfunction(lambda u, v: 3.0 + 4.0 * (u + v), (8, 8)).astype(np.float32)
+    xs = [torch.from_numpy(img).to(dev) for _ in range(2)]
+    ys = [torch.empty_like(xs[0]) for _ in range(2)]
+    stream = torch.cuda.Stream(device=dev)
+    bytes_step = 8.0 * h * w
+    out = {}
+    for name, q in (("sj", None), ("sj_quantized", steps_q)):
+        with torch.cuda.stream(stream):
+            for i in range(max(3, args.warmup)):
+                torch_api.image_blocks8(xs[i % 2], 0, quant=q, out=ys[i % 2])
+            stream.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=stream):
+                for i in range(args.steps):
+                    torch_api.image_blocks8(xs[i % 2], 0, quant=q, out=ys[i % 2])
+            if world > 1:
+                dist.barrier()
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            clk = Clocks(local)
+            with clk:
+                start.record(stream)
+                g.replay()
+                end.record(stream)
+                end.synchronize()
+        ms = max_over_ranks(start.elapsed_time(end), dev) / args.steps
+        out[name] = {"ms_per_step": ms, "gbs": bytes_step * world / (ms * 1e-3) / 1e9, "clocks": clk.summary()}
+        del g
+    # accuracy on a band of block rows against float64 per block
+    band = img[:512]
+    blocks = band.reshape(64, 8, 512, 8).transpose(0, 2, 1, 3).reshape(-1, 8, 8)
+    got = torch_api.image_blocks8(torch.from_numpy(band).to(dev), 0).cpu().numpy()
+    got_b = got.reshape(64, 8, 512, 8).transpose(0, 2, 1, 3).reshape(-1, 8, 8)
+    exact = O.fp64_apply(blocks.astype(np.float64), 0)
+    err = {"max_rel_err": O.rel_max_error(got_b, exact, blocks),
+           "max_rel_err_output_scaled": O.rel_max_error(got_b, exact, blocks, output_scaled=True),
+           "rms_rel_err": O.rel_rms_error(got_b, exact, blocks)}
+    # end to end from pinned host memory: copy in, transform, copy out, every step
+    hin = torch.from_numpy(img).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    e2e_steps = max(3, min(20, args.steps))
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            xs[0].copy_(hin, non_blocking=True)
+            torch_api.image_blocks8(xs[0], 0, out=ys[0])
+            hout.copy_(ys[0], non_blocking=True)
+        stream.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            xs[0].copy_(hin, non_blocking=True)
+            torch_api.image_blocks8(xs[0], 0, out=ys[0])
+            hout.copy_(ys[0], non_blocking=True)
+            stream.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dev)
+    e2e = {"value": bytes_step * e2e_steps * world / e2e_s / 1e9, "unit": "GB/s",
+           "h2d_bytes_per_step": int(4 * h * w), "d2h_bytes_per_step": int(4 * h * w),
+           "ms_per_step": 1e3 * e2e_s / e2e_steps, "path": "pinned copy in, one launch, copy out, serial"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = O.host_threads()
+        contiguous = img.reshape(512, 8, 512, 8).transpose(0, 2, 1, 3).reshape(-1, 8, 8).copy()
+        gbs, sample_txt = cpu_reference(contiguous, 0, threads, budget_s=2.0)
+        if gbs is not None:
+            cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "reference",
+                   "sample": sample_txt + "; the reference needs the blocks copied out contiguously first "
+                   "(not timed)"}
+    pk = peaks()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    head = out["sj"]
+    achieved = bytes_step / (head["ms_per_step"] * 1e-3) / 1e9
+    print(json.dumps({
+        "metric": METRIC, "value": head["gbs"], "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl["desc"], "shape": [h, w], "mode": "forward", "form": "sj",
+                   "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": "2 rotating input/output images (256 MiB) > L2",
+                   "timing": "CUDA events on the launch stream around CUDA-graph replays"},
+        "pct_hbm_peak": 100.0 * achieved / pk["hbm_gbs"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"], "traffic": None,
+                     "algorithmic_bytes_per_launch": bytes_step},
+        "forms": {**out, "sj": {**out["sj"], **err}}, "clocks": head["clocks"], "e2e": e2e,
+        "gpu_launches": args.steps, "cpu_baseline": cpu}))
 
 
 def launches_per_step(h: int, w: int, b: int) -> int:

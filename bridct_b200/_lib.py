@@ -77,6 +77,8 @@ EXTRA_SIGNATURES = [
     ("bridct_device_timeout_flag", C.c_int, [C.c_int]),
     ("bridct_ragged_apply_noalloc", C.c_int, [C.POINTER(RaggedItem), C.c_size_t, C.c_void_p, C.c_void_p,
                                               C.c_void_p]),
+    ("bridct_image_blocks8_device", C.c_int, [C.c_int, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_int,
+                                              C.c_int, C.c_void_p, C.c_void_p]),
 ]
 
 

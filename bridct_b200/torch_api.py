@@ -121,6 +121,34 @@ def roundtrip2(x: torch.Tensor) -> torch.Tensor:
     return apply(x, _lib.ROUNDTRIP)
 
 
+def image_blocks8(image: torch.Tensor, mode: int = 0, quant=None, out: torch.Tensor = None) -> torch.Tensor:
+    """Transforms every 8x8 block of a 2D float32 CUDA image where it lies (one launch).
+
+    `image` may be a strided view (row stride a multiple of 4, last stride 1); `quant` is an
+    optional 8x8 table of positive steps: forward returns rint(Y / Q), inverse dequantizes first,
+    roundtrip quantizes and dequantizes between the two.  `out` may be `image` itself.
+    """
+    if not (image.is_cuda and image.dtype == torch.float32 and image.dim() == 2 and image.stride(1) == 1):
+        raise ValueError("expected a 2D float32 CUDA tensor with unit column stride")
+    h, w = image.shape
+    if out is None:
+        out = torch.empty((h, w), dtype=torch.float32, device=image.device)
+    if out.shape != image.shape or out.stride(1) != 1 or out.device != image.device or out.dtype != torch.float32:
+        raise ValueError("out must be a float32 tensor of the image's shape on its device with unit column stride")
+    q = None
+    if quant is not None:
+        import numpy as np
+
+        qa = np.ascontiguousarray(np.asarray(quant, dtype=np.float32).reshape(64))
+        q = qa.ctypes.data
+    with torch.cuda.device(image.device):
+        st = _lib.lib().bridct_image_blocks8_device(mode, image.data_ptr(), image.stride(0), out.data_ptr(),
+                                                    out.stride(0), h, w, q,
+                                                    torch.cuda.current_stream().cuda_stream)
+    _lib.check(st, "bridct_image_blocks8_device")
+    return out
+
+
 class Plan:
     """Torch counterpart of bridct_numpy.Plan for CUDA tensors of one (height, width)."""
 

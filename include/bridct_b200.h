@@ -53,6 +53,19 @@ BRIDCT_API int bridct_plan_apply_form_device(bridct_plan *plan, enum bridct_mode
  * mbarrier wait expired (the kernel then skipped its remaining tiles and returned). */
 BRIDCT_API int bridct_device_timeout_flag(int device);
 
+/* ---- Block transform of an image in place-layout (codec step) ------------------------- */
+
+/* Transforms every 8x8 block of a height x width float32 image where it lies (row pitches in
+ * floats, multiples of 4; 16-byte aligned device pointers; output may equal input with the
+ * same pitch).  quant: NULL, or 64 positive quantization steps in host memory (row-major 8x8):
+ * FORWARD then writes rint(Y / Q), INVERSE multiplies its input by Q before the DCT-III, and
+ * ROUNDTRIP quantizes and dequantizes between the two.  Asynchronous on `stream` (NULL = CUDA
+ * default stream); allocates nothing.  The reference has no strided or in-image entry point
+ * (docs/API.md:17 requires contiguous arrays): callers there copy each block out and back. */
+BRIDCT_API int bridct_image_blocks8_device(int mode, const float *input, size_t input_pitch,
+                                           float *output, size_t output_pitch, int height, int width,
+                                           const float *quant, void *stream);
+
 /* ---- Batching form: mixed shapes and directions in one persistent launch ---------------- */
 
 /* One array of a ragged batch: shape, mode (enum bridct_mode) and offset, in floats, from the
