@@ -333,7 +333,8 @@ def main():
 
     forms = {"sj": _lib.FORM_SJ}
     if args.form in ("auto",):
-        for name, fid in (("tc_bf16x3", _lib.FORM_TC_BF16X3), ("tc_tf32x3", _lib.FORM_TC_TF32X3)):
+        for name, fid in (("tc_bf16x3", _lib.FORM_TC_BF16X3), ("tc_tf32x3", _lib.FORM_TC_TF32X3),
+                          ("tc_fp8", _lib.FORM_TC_FP8)):
             probe = lib.bridct_plan_apply_form_device(plan, mode, fid, xs[0].data_ptr(), ys[0].data_ptr(), b,
                                                       stream.cuda_stream)
             if probe == 0:

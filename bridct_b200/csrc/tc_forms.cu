@@ -15,6 +15,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -27,6 +28,7 @@
 #include "tc_blocks8.cuh"
 #include "tc_pass.cuh"
 #include "tc_fused64.cuh"
+#include "tc_fp8.cuh"
 
 namespace bridct {
 namespace {
@@ -125,6 +127,8 @@ std::vector<uint8_t> b_image(int form, bool inverse) {
 struct TcDevice {
   void* images[3][2] = {};   // [form][inverse]
   void* pass_images[3][3][2] = {};   // [form][log2(L) - 6][inverse], built on first use
+  void* fp8_images[2][2] = {};       // [L == 256][inverse]: E4M3 codes of C or C^T
+  float* fp8_scales[2][2] = {};      // their 32x32 tile scales
   int* err = nullptr;
 };
 
@@ -206,6 +210,53 @@ bool make_map(CUtensorMap* m, const float* ptr, size_t rows) {
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Value of E4M3 code c (1 sign, 4 exponent bits with bias 7, 3 mantissa bits; 0x7F is NaN).
+double e4m3_value(int c) {
+  const int e = (c >> 3) & 15, m = c & 7;
+  const double mag = e == 0 ? m * std::ldexp(1.0, -9) : (1.0 + m / 8.0) * std::ldexp(1.0, e - 7);
+  return (c & 0x80) ? -mag : mag;
+}
+
+// Nearest E4M3 code to v (ties to the even code), saturating at +-448.
+uint8_t e4m3_encode(double v) {
+  const double a = std::fabs(v);
+  int best = 0;
+  double bd = a;
+  for (int c = 1; c <= 0x7E; ++c) {
+    const double d = std::fabs(e4m3_value(c) - a);
+    if (d < bd || (d == bd && (c & 1) == 0)) {
+      best = c;
+      bd = d;
+    }
+  }
+  return (uint8_t)(best | (v < 0 && best ? 0x80 : 0));
+}
+
+// E4M3 image of C_L (forward) or C_L^T for the FP8 pass: slice nb (64 rows) at nb * 64 * L bytes,
+// laid out [K atom of 128][64 rows x 128 bytes, SW128]; scales [L/32 row bands][L/32 K-tiles].
+void fp8_image(int L, bool inverse, std::vector<uint8_t>& img, std::vector<float>& sc) {
+  const std::vector<double> c = dct_matrix(L);
+  auto at = [&](int n, int k) { return inverse ? c[(size_t)k * L + n] : c[(size_t)n * L + k]; };
+  const int nt = L / 32;
+  sc.assign((size_t)nt * nt, 1.0f);
+  img.assign((size_t)L * L, 0);
+  for (int bn = 0; bn < nt; ++bn)
+    for (int bk = 0; bk < nt; ++bk) {
+      double amax = 0.0;
+      for (int i = 0; i < 32; ++i)
+        for (int j = 0; j < 32; ++j) amax = std::max(amax, std::fabs(at(bn * 32 + i, bk * 32 + j)));
+      const float s = amax > 0 ? (float)(amax / tc::kE4M3Max) : 1.0f;
+      sc[(size_t)bn * nt + bk] = s;
+      for (int i = 0; i < 32; ++i)
+        for (int j = 0; j < 32; ++j) {
+          const int n = bn * 32 + i, k = bk * 32 + j;
+          const size_t slice = (size_t)(n / 64) * 64 * L;
+          const size_t off = slice + (size_t)(k / 128) * 8192 + tc::sw128(n % 64, (k % 128) / 16) + (k % 16);
+          img[off] = e4m3_encode(at(n, k) / s);
+        }
+    }
+}
+
 // Row matrix (rows x L FP32) viewed by TMA in boxes of 32 x 128, 128-byte swizzle.
 bool make_rows_map(CUtensorMap* m, const float* ptr, size_t rows, int L) {
   EncodeTiledFn enc = encode_fn();
@@ -282,6 +333,148 @@ int launch_fused64(const bridct_plan* p, bool inverse, const float* x, float* y,
   tc::k_tc64<<<(unsigned)grid, F::kThreads, F::kDynamic, st>>>(xm, y, img, (long long)batch, d->err);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_tc64 launch");
+}
+
+// ---- FP8 form ---------------------------------------------------------------------------
+
+int log2i(int v);
+
+bool make_fp8_map(CUtensorMap* m, const uint8_t* ptr, size_t rows, int L) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)L, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)L};
+  cuuint32_t box[2] = {128, tc::kRows};
+  cuuint32_t estr[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(ptr), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool fp8_tables(TcDevice* d, int L, bool inverse, const uint4** img, const float** sc) {
+  std::lock_guard<std::mutex> lock(g_tc_mutex);
+  const int li = L == 256 ? 1 : 0, iv = inverse ? 1 : 0;
+  if (!d->fp8_images[li][iv]) {
+    std::vector<uint8_t> im;
+    std::vector<float> scl;
+    fp8_image(L, inverse, im, scl);
+    void* pi = nullptr;
+    void* ps = nullptr;
+    if (cudaMalloc(&pi, im.size()) != cudaSuccess || cudaMalloc(&ps, scl.size() * 4) != cudaSuccess) return false;
+    if (cudaMemcpy(pi, im.data(), im.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(ps, scl.data(), scl.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+      return false;
+    d->fp8_images[li][iv] = pi;
+    d->fp8_scales[li][iv] = static_cast<float*>(ps);
+  }
+  *img = reinterpret_cast<const uint4*>(d->fp8_images[li][iv]);
+  *sc = d->fp8_scales[li][iv];
+  return true;
+}
+
+template <int L>
+int launch_fp8pass(const bridct_plan* p, bool inverse, const uint8_t* q, const float* sx, float* out, size_t rows,
+                   int rshift, cudaStream_t st, TcDevice* d) {
+  using F = tc::Fp8Layout<L>;
+  auto k = tc::k_fp8pass<L>;
+  static const bool attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, F::kDynamic) ==
+                           cudaSuccess;
+  if (!attr) return cuda_fail(cudaErrorInvalidConfiguration, "k_fp8pass shared memory");
+  const uint4* img = nullptr;
+  const float* sc = nullptr;
+  if (!fp8_tables(d, L, inverse, &img, &sc)) return cuda_fail(cudaGetLastError(), "FP8 coefficient upload");
+  CUtensorMap m;
+  if (!make_fp8_map(&m, q, rows, L)) {
+    set_error("cuTensorMapEncodeTiled failed");
+    return BRIDCT_DEVICE_ERROR;
+  }
+  constexpr int kBlocks = L / 64;
+  const long long mtiles = (long long)((rows + tc::kRows - 1) / tc::kRows);
+  long long slots = p->dev->sm_count / kBlocks;
+  if (slots > mtiles) slots = mtiles;
+  if (slots < 1) slots = 1;
+  k<<<(unsigned)(slots * kBlocks), F::kThreads, F::kDynamic, st>>>(m, sx, out, img, sc, (long long)rows, rshift,
+                                                                    d->err);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_fp8pass launch");
+}
+
+// Quantizes the rows (nrows x L, 32-row bands) into E4M3 codes q and tile scales sx.
+int launch_quant8(const float* rows, uint8_t* q, float* sx, size_t nrows, int L, cudaStream_t st) {
+  const long long ntiles = (long long)(nrows / 32) * (L / 32);
+  tc::k_quant8<<<(unsigned)((ntiles + 7) / 8), 256, 0, st>>>(rows, q, sx, ntiles, L);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_quant8 launch");
+}
+
+struct Fp8Scratch {
+  float *t, *r, *r2, *z, *sx;
+  uint8_t* q;
+};
+
+// Unrefined FP8 transform of nb arrays: quantize, pass over rows of W, quantize, pass over rows of H.
+int fp8_transform(const bridct_plan* p, bool inverse, const float* src, float* dst, size_t nb, const Fp8Scratch& s,
+                  cudaStream_t st, TcDevice* d) {
+  const int h = p->h, w = p->w;
+  auto pass = [&](int L, const uint8_t* q, const float* sx, float* out, size_t rows, int rshift) {
+    return L == 128 ? launch_fp8pass<128>(p, inverse, q, sx, out, rows, rshift, st, d)
+                    : launch_fp8pass<256>(p, inverse, q, sx, out, rows, rshift, st, d);
+  };
+  int e = launch_quant8(src, s.q, s.sx, nb * h, w, st);
+  if (!e) e = pass(w, s.q, s.sx, s.t, nb * h, log2i(h));
+  if (!e) e = launch_quant8(s.t, s.q, s.sx, nb * w, h, st);
+  if (!e) e = pass(h, s.q, s.sx, dst, nb * w, log2i(w));
+  return e;
+}
+
+// One refinement step: dst = T8(src) + T8(src - T32^-1(T8(src))), with the plain FP32 form for
+// the inverse and the residual in FP32.  src and dst must differ.
+int fp8_refined(const bridct_plan* p, bool inverse, const float* src, float* dst, size_t nb, const Fp8Scratch& s,
+                cudaStream_t st, TcDevice* d) {
+  const long long n4 = (long long)(nb * p->elements / 4);
+  const unsigned grid = (unsigned)std::min<long long>((n4 + 255) / 256, 4 * 148);
+  int e = fp8_transform(p, inverse, src, dst, nb, s, st, d);
+  if (!e) e = launch_plain_form(p, inverse ? 0 : 1, dst, s.r, (long long)nb, st);
+  if (e) return e;
+  tc::k_residual<<<grid, 256, 0, st>>>(reinterpret_cast<const float4*>(src), reinterpret_cast<float4*>(s.r), n4);
+  e = fp8_transform(p, inverse, s.r, s.r2, nb, s, st, d);
+  if (e) return e;
+  tc::k_accumulate<<<grid, 256, 0, st>>>(reinterpret_cast<float4*>(dst), reinterpret_cast<const float4*>(s.r2), n4);
+  cudaError_t ce = cudaGetLastError();
+  return ce == cudaSuccess ? BRIDCT_OK : cuda_fail(ce, "FP8 refinement");
+}
+
+int apply_fp8(bridct_plan* p, int mode, const float* x, float* y, size_t batch, cudaStream_t st, TcDevice* d) {
+  const size_t elems = p->elements;
+  size_t chunk = (size_t(16) << 20) / (elems * sizeof(float));
+  if (chunk < 1) chunk = 1;
+  if (chunk > batch) chunk = batch;
+  const size_t ce = chunk * elems;
+  const size_t need = 16 * ce + ce + 4 * (ce / 1024) + 4096;
+  if (p->tc_bytes < need) {
+    if (p->tc_mem) cudaFree(p->tc_mem);
+    p->tc_mem = nullptr;
+    p->tc_bytes = 0;
+    cudaError_t e = cudaMalloc(&p->tc_mem, need);
+    if (e != cudaSuccess) return cuda_fail(e, "FP8 scratch");
+    p->tc_bytes = need;
+  }
+  float* base = static_cast<float*>(p->tc_mem);
+  Fp8Scratch s{base, base + ce, base + 2 * ce, base + 3 * ce, base + 4 * ce, nullptr};
+  s.q = reinterpret_cast<uint8_t*>(s.sx + ce / 1024 + 256);
+  for (size_t b0 = 0; b0 < batch; b0 += chunk) {
+    const size_t nb = batch - b0 < chunk ? batch - b0 : chunk;
+    const float* xc = x + b0 * elems;
+    float* yc = y + b0 * elems;
+    int e = fp8_refined(p, mode == 1, xc, yc, nb, s, st, d);
+    if (!e && mode == 2) {
+      e = fp8_refined(p, true, yc, s.z, nb, s, st, d);
+      if (!e && cudaMemcpyAsync(yc, s.z, nb * elems * sizeof(float), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        e = cuda_fail(cudaGetLastError(), "FP8 round trip copy");
+    }
+    if (e) return e;
+  }
+  return BRIDCT_OK;
 }
 
 template <int FORM>
@@ -374,8 +567,12 @@ int launch_tc8(const bridct_plan* p, int inverse, const float* x, float* y, size
 
 int apply_tc_form(bridct_plan* p, int mode, int form, const float* x, float* y, size_t batch, void* stream) {
   if (!p || !x || !y || mode < 0 || mode > 2 || batch == 0) return BRIDCT_INVALID_ARGUMENT;
-  if (form != BRIDCT_FORM_TC_BF16X3 && form != BRIDCT_FORM_TC_TF32X3) {
+  if (form != BRIDCT_FORM_TC_BF16X3 && form != BRIDCT_FORM_TC_TF32X3 && form != BRIDCT_FORM_TC_FP8) {
     set_error("unsupported execution form");
+    return BRIDCT_INVALID_ARGUMENT;
+  }
+  if (form == BRIDCT_FORM_TC_FP8 && !((p->h == 128 || p->h == 256) && (p->w == 128 || p->w == 256))) {
+    set_error("the FP8 form covers arrays whose axes are 128 or 256");
     return BRIDCT_INVALID_ARGUMENT;
   }
   const bool sep_axis_h = p->h == 64 || p->h == 128 || p->h == 256;
@@ -394,6 +591,7 @@ int apply_tc_form(bridct_plan* p, int mode, int form, const float* x, float* y, 
   TcDevice* d = tc_device(p->device);
   if (!d) return cuda_fail(cudaGetLastError(), "tensor-core setup");
   cudaStream_t st = (cudaStream_t)stream;
+  if (form == BRIDCT_FORM_TC_FP8) return apply_fp8(p, mode, x, y, batch, st, d);
   if (!kron)
     return form == BRIDCT_FORM_TC_BF16X3 ? apply_sep<tc::BF16X3>(p, mode, x, y, batch, st, d)
                                         : apply_sep<tc::TF32X3>(p, mode, x, y, batch, st, d);

@@ -156,3 +156,45 @@ def test_tc64_fused_batches(batch):
     for mode in range(3):
         y = run(x, mode, "tc_bf16x3")
         assert O.rel_max_error(y, O.fp64_apply(x, mode), x, output_scaled=True) <= TOL, (batch, mode)
+
+
+# FP8 E4M3 with 32x32 tile scales plus one FP32 refinement step.  A float64 emulation of the
+# same quantization gives, on U[-1,1] 256x256 arrays, max 6.0e-2 / RMS 2.8e-2 before and
+# max 2.7e-3 / RMS 1.5e-3 after the refinement; the bounds below are about 4x those.
+FP8_MAX, FP8_RMS = 1e-2, 5e-3
+
+
+@pytest.mark.parametrize("shape", [(128, 128), (256, 256), (128, 256), (256, 128)])
+def test_fp8_refined_error(shape):
+    x = np.random.default_rng(shape[0] + 3 * shape[1]).uniform(-1, 1, (3, *shape)).astype(np.float32)
+    for mode in range(3):
+        y = run(x, mode, "tc_fp8")
+        ref = O.fp64_apply(x, mode)
+        k = 2.0 if mode == 2 else 1.0
+        assert O.rel_max_error(y, ref, x, output_scaled=True) <= k * FP8_MAX, (shape, mode)
+        assert O.rel_rms_error(y, ref, x) <= k * FP8_RMS, (shape, mode)
+
+
+def test_fp8_impulse_constant_and_batch_edges():
+    x = np.zeros((5, 256, 256), np.float32)
+    x[0, 3, 250] = 1.0
+    x[1] = -7.5e-4
+    x[2:] = np.random.default_rng(11).standard_normal((3, 256, 256)) * 1e4
+    y = run(x, 0, "tc_fp8")
+    ref = O.fp64_apply(x, 0)
+    for i in range(5):
+        assert O.rel_max_error(y[i:i + 1], ref[i:i + 1], x[i:i + 1], output_scaled=True) <= FP8_MAX, i
+
+
+def test_fp8_no_write_past_batch_and_rejects_other_shapes():
+    L = _lib.lib()
+    plan = torch_api._plan(torch.cuda.current_device(), 128, 256)
+    x = torch.randn(4, 128, 256, device="cuda")
+    y = torch.full_like(x, 12345.0)
+    assert L.bridct_plan_apply_form_device(plan, 0, _lib.FORM_TC_FP8, x.data_ptr(), y.data_ptr(), 3, None) == 0
+    torch.cuda.synchronize()
+    assert (y[3] == 12345.0).all() and torch.isfinite(y[:3]).all()
+    plan64 = torch_api._plan(torch.cuda.current_device(), 64, 64)
+    z = torch.randn(2, 64, 64, device="cuda")
+    assert L.bridct_plan_apply_form_device(plan64, 0, _lib.FORM_TC_FP8, z.data_ptr(), z.data_ptr() + 0, 1,
+                                           None) in (_lib.INVALID_ARGUMENT, _lib.OVERLAPPING_BUFFERS)
