@@ -5,7 +5,7 @@
 Steps: regenerate csrc/sj_generated.cuh from csrc/gen_sj.py when the generator changed,
 compile each CUDA translation unit with nvcc (-gencode arch=compute_100a,code=sm_100a), the
 plain-form instantiations once per array height in parallel, and link one shared library
-with the CUDA runtime linked statically.  Objects go to _build/ at the repository root.
+with the CUDA runtime linked statically; then build the pipe runner against it.  Objects go to _build/ at the repository root.
 """
 from __future__ import annotations
 
@@ -21,6 +21,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT = ROOT / "_build"
 LIB = PKG / "libbridct_b200.so"
+RUNNER = PKG / "bridct_runner"
 HEIGHTS = (8, 16, 32, 64, 128, 256, 512, 1024)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
@@ -77,6 +78,12 @@ def build(verbose: bool = False) -> Path:
     objs = [o for o, _, _ in jobs]
     if _newer(LIB, objs):
         _run([nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", str(LIB)] + [str(o) for o in objs])
+    # the pipe runner (wire protocol of the reference's test runner) next to the library
+    runner_src = PKG / "runner" / "bridct_runner.c"
+    if _newer(RUNNER, [runner_src, LIB, ROOT / "include" / "bridct.h"]):
+        cc = os.environ.get("CC") or shutil.which("gcc") or "cc"
+        _run([cc, "-std=c11", "-O2", "-Wall", "-I", str(ROOT / "include"), str(runner_src), "-L", str(PKG),
+              "-l:libbridct_b200.so", "-Wl,-rpath,$ORIGIN", "-o", str(RUNNER)])
     if verbose:
         print(f"built {LIB}")
     return LIB
