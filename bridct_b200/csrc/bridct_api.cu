@@ -12,6 +12,7 @@
 // launcher table) created on first use; each plan owns a CUDA stream plus device and
 // pinned staging for host-pointer calls.
 #include <cuda_runtime.h>
+#include <tuple>
 
 #include <algorithm>
 #include <cmath>
@@ -208,6 +209,28 @@ static bool ranges_overlap(uintptr_t a, size_t na, uintptr_t b, size_t nb) {
 }  // namespace bridct
 
 using namespace bridct;
+
+namespace bridct {
+
+int kernel_setup(const void* kernel, int smem, int threads) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, int, int>, int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  const auto key = std::make_tuple(kernel, dev, smem, threads);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int blocks = 0;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+    return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, smem) != cudaSuccess) return 0;
+  cache[key] = blocks;
+  return blocks;
+}
+
+}  // namespace bridct
 
 extern "C" {
 

@@ -29,6 +29,10 @@ double sj_scale(int n, int k);
 void build_fourstep_tables(int N, std::vector<float2>& tw, std::vector<float4>& post);
 void fill_fourstep_tables(int N, float2* tw, float4* post);
 DeviceCtx* device_ctx(int device);
+// Opts `kernel` into `smem` bytes of dynamic shared memory on the current device and returns
+// its resident blocks per SM at `threads` threads (0 on failure); cached per device, since the
+// attribute belongs to the device's copy of the kernel.
+int kernel_setup(const void* kernel, int smem, int threads);
 int current_device(int* dev);
 const void* device_address(const void* p, bool* pinned);
 

@@ -14,16 +14,12 @@ struct LaunchCtx {
 using PlainLauncher = cudaError_t (*)(const float*, float*, long long, cudaStream_t,
                                       LineTables, const LaunchCtx&);
 
-// Blocks per SM for a kernel at a given dynamic shared-memory size (computed once).
+int kernel_setup(const void* kernel, int smem, int threads);   // bridct_api.cu
+
+// Blocks per SM for a kernel at a given dynamic shared-memory size (set up once per device).
 template <typename Kernel>
-static int kernel_blocks_per_sm(Kernel k, int smem) {
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return 0;
-  }
-  int b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kThreads, smem) != cudaSuccess) return 0;
-  return b;
+static int kernel_blocks_per_sm(Kernel k, int smem, int threads = kThreads) {
+  return kernel_setup(reinterpret_cast<const void*>(k), smem, threads);
 }
 
 template <typename Kernel>
@@ -45,7 +41,7 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
   if constexpr (H == 8 && W == 8) {
     auto k = k_blocks8<MODE>;
     constexpr int smem = kB8Chunks * 16;
-    static const int bps = kernel_blocks_per_sm(k, smem);
+    const int bps = kernel_blocks_per_sm(k, smem, kB8Threads);
     if (bps <= 0) return cudaErrorInvalidConfiguration;
     const long long ntiles = (batch + kB8Threads - 1) / kB8Threads;
     long long grid = (long long)ctx.sm_count * bps;
@@ -54,14 +50,14 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
     return cudaGetLastError();
   } else if constexpr (Gm::kTile) {
     auto k = k_full<H, W, Gm::kTR, true, true, MODE>;
-    static const int bps = kernel_blocks_per_sm(k, Gm::kSmemFull);
+    const int bps = kernel_blocks_per_sm(k, Gm::kSmemFull);
     TileArgs a{x, y, (batch * H + Gm::kTR - 1) / Gm::kTR, batch * H, tab};
     return launch_tiles(k, Gm::kSmemFull, bps, a, ctx, st);
   } else {
     auto kc = k_colstrip<H, W, Gm::kTC, MODE>;
     auto kr = k_full<H, W, Gm::kRB, false, true, MODE>;
-    static const int bpc = kernel_blocks_per_sm(kc, Gm::kSmemStrip);
-    static const int bpr = kernel_blocks_per_sm(kr, Gm::kSmemRows);
+    const int bpc = kernel_blocks_per_sm(kc, Gm::kSmemStrip);
+    const int bpr = kernel_blocks_per_sm(kr, Gm::kSmemRows);
     const long long bytes = (long long)H * W * 4;
     long long chunk = ctx.l2_chunk_bytes / bytes;
     if (chunk < 1) chunk = 1;

@@ -189,13 +189,7 @@ BRIDCT_API bridct_ragged* bridct_ragged_create_tuned(const bridct_ragged_item* i
     bridct_ragged_destroy(r);
     return nullptr;
   }
-  static int bps = [] {
-    if (cudaFuncSetAttribute(k_ragged, cudaFuncAttributeMaxDynamicSharedMemorySize, kRaggedSmem) != cudaSuccess)
-      return 0;
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_ragged, kRaggedThreads, kRaggedSmem) != cudaSuccess) return 0;
-    return b;
-  }();
+  const int bps = kernel_setup(reinterpret_cast<const void*>(k_ragged), kRaggedSmem, kRaggedThreads);
   if (bps <= 0) {
     cuda_fail(cudaErrorInvalidConfiguration, "k_ragged occupancy");
     bridct_ragged_destroy(r);
@@ -432,13 +426,7 @@ extern "C" BRIDCT_API int bridct_ragged_apply_noalloc(const bridct_ragged_item* 
     if (e != cudaSuccess) return cuda_fail(e, "scratch tables");
     g_na_addr[dev] = base;
   }
-  static int bps = [] {
-    if (cudaFuncSetAttribute(k_ragged, cudaFuncAttributeMaxDynamicSharedMemorySize, kRaggedSmem) != cudaSuccess)
-      return 0;
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_ragged, kRaggedThreads, kRaggedSmem) != cudaSuccess) return 0;
-    return b;
-  }();
+  const int bps = kernel_setup(reinterpret_cast<const void*>(k_ragged), kRaggedSmem, kRaggedThreads);
   int sms = 0;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess || bps <= 0) return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidConfiguration, "k_ragged");

@@ -294,9 +294,8 @@ int launch_pass(const bridct_plan* p, bool inverse, const float* x, float* out, 
                 cudaStream_t st, TcDevice* d) {
   using PL = tc::PassLayout<FORM, L>;
   auto k = tc::k_tcpass<FORM, L>;
-  static const bool attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                PL::kDynamic) == cudaSuccess;
-  if (!attr) return cuda_fail(cudaErrorInvalidConfiguration, "k_tcpass shared memory");
+  if (kernel_setup(reinterpret_cast<const void*>(k), PL::kDynamic, tc::kWsThreads) <= 0)
+    return cuda_fail(cudaErrorInvalidConfiguration, "k_tcpass shared memory");
   const uint4* img = pass_image_device<FORM, L>(d, inverse);
   if (!img) return cuda_fail(cudaGetLastError(), "tensor-core coefficient upload");
   CUtensorMap xm;
@@ -318,9 +317,8 @@ int launch_pass(const bridct_plan* p, bool inverse, const float* x, float* out, 
 int launch_fused64(const bridct_plan* p, bool inverse, const float* x, float* y, size_t batch, cudaStream_t st,
                    TcDevice* d) {
   using F = tc::Fused64;
-  static const bool attr =
-      cudaFuncSetAttribute(tc::k_tc64, cudaFuncAttributeMaxDynamicSharedMemorySize, F::kDynamic) == cudaSuccess;
-  if (!attr) return cuda_fail(cudaErrorInvalidConfiguration, "k_tc64 shared memory");
+  if (kernel_setup(reinterpret_cast<const void*>(tc::k_tc64), F::kDynamic, F::kThreads) <= 0)
+    return cuda_fail(cudaErrorInvalidConfiguration, "k_tc64 shared memory");
   const uint4* img = pass_image_device<tc::BF16X3, 64>(d, inverse);
   if (!img) return cuda_fail(cudaGetLastError(), "tensor-core coefficient upload");
   CUtensorMap xm;
@@ -377,9 +375,8 @@ int launch_fp8pass(const bridct_plan* p, bool inverse, const uint8_t* q, const f
                    int rshift, cudaStream_t st, TcDevice* d) {
   using F = tc::Fp8Layout<L>;
   auto k = tc::k_fp8pass<L>;
-  static const bool attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, F::kDynamic) ==
-                           cudaSuccess;
-  if (!attr) return cuda_fail(cudaErrorInvalidConfiguration, "k_fp8pass shared memory");
+  if (kernel_setup(reinterpret_cast<const void*>(k), F::kDynamic, F::kThreads) <= 0)
+    return cuda_fail(cudaErrorInvalidConfiguration, "k_fp8pass shared memory");
   const uint4* img = nullptr;
   const float* sc = nullptr;
   if (!fp8_tables(d, L, inverse, &img, &sc)) return cuda_fail(cudaGetLastError(), "FP8 coefficient upload");
@@ -542,12 +539,7 @@ int launch_tc8(const bridct_plan* p, int inverse, const float* x, float* y, size
                TcDevice* d) {
   using L = tc::Layout<FORM>;
   auto k = tc::k_tc8<FORM>;
-  static const int bps = [&]() {
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kDynamic) != cudaSuccess) return 0;
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, tc::kWsThreads, L::kDynamic) != cudaSuccess) return 0;
-    return b;
-  }();
+  const int bps = kernel_setup(reinterpret_cast<const void*>(k), L::kDynamic, tc::kWsThreads);
   if (bps <= 0) return cuda_fail(cudaErrorInvalidConfiguration, "k_tc8 occupancy");
   CUtensorMap xm, ym;
   if (!make_map(&xm, x, batch) || !make_map(&ym, y, batch)) {
