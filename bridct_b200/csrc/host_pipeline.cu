@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstring>
 #include <map>
+#include <vector>
 
 #include "../../include/bridct.h"
 #include "../../include/bridct_b200.h"
@@ -69,9 +70,25 @@ int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, s
   bool used[kSlots] = {}, pending[kSlots] = {};
   cudaError_t e = cudaSuccess;
   size_t ci = 0;
-  for (size_t a0 = 0; a0 < batch; a0 += chunk, ++ci) {
+  // Chunk sizes ramp up at the start (1/4, 1/2, full) and down at the end (1/2, 1/4): the first
+  // copy in and the last copy out overlap nothing, so they are kept short.
+  std::vector<size_t> sizes;
+  {
+    const size_t q = chunk / 4, h = chunk / 2;
+    if (q >= 1 && batch >= 2 * (q + h) + 2 * chunk) {
+      size_t mid = batch - 2 * (q + h);
+      sizes = {q, h};
+      for (; mid > chunk; mid -= chunk) sizes.push_back(chunk);
+      sizes.push_back(mid);
+      sizes.push_back(h);
+      sizes.push_back(q);
+    } else {
+      for (size_t a = 0; a < batch; a += chunk) sizes.push_back(batch - a < chunk ? batch - a : chunk);
+    }
+  }
+  size_t a0 = 0;
+  for (size_t na : sizes) {
     const int slot = (int)(ci % kSlots);
-    const size_t na = batch - a0 < chunk ? batch - a0 : chunk;
     const size_t off = a0 * per, nbytes = na * per * sizeof(float);
     float* sx = p->d_batch + (size_t)slot * 2 * cf;
     float* sy = sx + cf;
@@ -135,6 +152,8 @@ int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, s
       if (e != cudaSuccess) return cuda_fail(e, "batch D2H");
     }
     used[slot] = true;
+    a0 += na;
+    ++ci;
   }
   for (int i = 0; i < 3; ++i) {
     e = cudaStreamSynchronize(p->aux[i]);
