@@ -181,11 +181,11 @@ __global__ void __launch_bounds__(kThreads) k_full(TileArgs a) {
     const long long left = a.rows_total - t * (long long)TR;
     return left >= TR ? TR : (int)left;
   };
-  // Whole-array tiles with a four-step axis are latency-bound: they prefetch the next tile into
-  // registers during the transform (measured +20-50% on such shapes).  Register-line kernels and
-  // the row pass of the two-pass route keep their occupancy instead (prefetching cost them up to
-  // 18%).
-  constexpr bool kPrefetch = DO_COL && DO_ROW && (H >= 128 || W >= 128);
+  // Whole-array tiles with a four-step axis, and row passes of 128..512-point lines, are
+  // latency-bound: they prefetch the next tile into registers during the transform (measured
+  // +10-50% on such shapes).  Register-line kernels and 1024-point rows keep their occupancy
+  // instead (prefetching cost them up to 18%).
+  constexpr bool kPrefetch = DO_COL ? DO_ROW && (H >= 128 || W >= 128) : (DO_ROW && W >= 128 && W <= 512);
   TileRegs<P, kPrefetch ? TR : 4, kPrefetch ? W : 4> next;
   if (kPrefetch && blockIdx.x < a.ntiles) next.load(a.x + blockIdx.x * (long long)TR * W, W, rows_of(blockIdx.x));
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
@@ -222,11 +222,23 @@ __global__ void __launch_bounds__(kThreads) k_colstrip(TileArgs a) {
   float* tile = smem;
   float* xbuf = smem + round4(H * P);
   const FourStepTables tcol = stage_tables<H>(a.tab.col, xbuf + round4(kWarps * ExchangeFloats<H>::value));
+  // Strips of 128- and 256-point columns prefetch the next strip into registers during the
+  // transform; longer columns keep their occupancy.
+  constexpr bool kPrefetch = H == 128 || H == 256;
+  auto src = [&](long long t) { return a.x + (t / STRIPS) * (long long)H * W + (t % STRIPS) * TC; };
+  TileRegs<P, kPrefetch ? H : 4, kPrefetch ? TC : 4> next;
+  if (kPrefetch && blockIdx.x < a.ntiles) next.load(src(blockIdx.x), W, H);
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const long long arr = t / STRIPS;
     const int s = (int)(t % STRIPS);
-    tile_load<P>(a.x + arr * (long long)H * W + s * TC, W, H, TC, tile, H);
-    __syncthreads();
+    if constexpr (kPrefetch) {
+      next.put(tile);
+      __syncthreads();
+      if (t + gridDim.x < a.ntiles) next.load(src(t + gridDim.x), W, H);
+    } else {
+      tile_load<P>(a.x + arr * (long long)H * W + s * TC, W, H, TC, tile, H);
+      __syncthreads();
+    }
     run_lines<H, MODE>(tile, TC, P, [](int l) { return l; }, xbuf, tcol);
     __syncthreads();
     tile_store<P>(a.y + arr * (long long)H * W + s * TC, W, H, TC, tile);
