@@ -199,8 +199,13 @@ def run_reference_arm(args, rank: int, world: int):
         return
     wl = workload(args.workload)
     x = wl["x"]
-    b, h, w = x.shape
     threads = O.host_threads()
+    if "items" in wl:
+        return _reference_ragged(args, wl, world, threads)
+    if x.ndim == 2:   # image workload: the reference needs the blocks copied out contiguously (untimed)
+        x = np.ascontiguousarray(x.reshape(x.shape[0] // 8, 8, x.shape[1] // 8, 8).transpose(0, 2, 1, 3)
+                                 .reshape(-1, 8, 8))
+    b, h, w = x.shape
     line = {"metric": METRIC, "unit": "GB/s", "impl": "reference", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
@@ -221,6 +226,41 @@ def run_reference_arm(args, rank: int, world: int):
     line["config"]["sample_arrays_per_step"] = n
     line["cpu_baseline"] = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "reference",
                             "sample": f"{n} of {b} arrays per step, {threads} threads, one plan per thread"}
+    line["e2e"] = {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    print(json.dumps(line))
+
+
+def _reference_ragged(args, wl, world, threads):
+    """Reference arm on the mixed batch: the same arrays, one reference plan per shape and thread."""
+    from oracle import oracle as O
+
+    items = wl["items"]
+    hs = np.array([h for h, _, _ in items], np.int32)
+    ws = np.array([w for _, w, _ in items], np.int32)
+    modes = np.array([m for _, _, m in items], np.int32)
+    offs = np.concatenate([[0], np.cumsum(hs.astype(np.int64) * ws)[:-1]]).astype(np.uint64)
+    x = wl["x"]
+    y = np.empty_like(x)
+    line = {"metric": METRIC, "unit": "GB/s", "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": {"workload": wl["desc"], "arrays": len(items)}}
+    if not O.bench_available():
+        line["unavailable"] = "reference library not built (oracle/_ref missing)"
+        print(json.dumps(line))
+        return
+    # the first n arrays (the list is in random order) so that one pass takes about per_step seconds
+    per_step = min(0.5, 60.0 / max(1, args.steps + args.warmup))
+    n0 = min(len(items), 64)
+    t0 = O.ref_bench(hs[:n0], ws[:n0], modes[:n0], offs[:n0], x, y, threads, 1)
+    n = int(min(len(items), max(n0, n0 * per_step / max(t0, 1e-9))))
+    if args.warmup:
+        O.ref_bench(hs[:n], ws[:n], modes[:n], offs[:n], x, y, threads, args.warmup)
+    total = O.ref_bench(hs[:n], ws[:n], modes[:n], offs[:n], x, y, threads, args.steps)
+    gbs = 8.0 * float((hs[:n].astype(np.int64) * ws[:n]).sum()) * args.steps / total / 1e9
+    line.update(value=gbs, ms_per_step=1e3 * total / args.steps)
+    line["config"]["sample_arrays_per_step"] = n
+    line["cpu_baseline"] = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "reference",
+                            "sample": f"first {n} of {len(items)} arrays per step, {threads} threads"}
     line["e2e"] = {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     print(json.dumps(line))
 
