@@ -2,7 +2,7 @@
 tensor-core split-precision forms, with the reference's own CPU path timed on the host.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload blocks8|image8|arrays64|large1024|ragged|sweep256] [--form auto|sj|...]
+                    [--workload blocks8|image8|arrays64|large1024|ragged|sweep256|shapes] [--form auto|sj|...]
 
 Default workload: 262,144 independent 8x8 blocks of a 4096x4096 image (pixels uniform integers
 0..255 minus 128, seed 1), forward DCT-II, blocks stored contiguously as (B, 8, 8).  A step is
@@ -56,6 +56,9 @@ def workload(name: str):
         x = img.reshape(512, 8, 512, 8).transpose(0, 2, 1, 3).reshape(-1, 8, 8).copy()
         return dict(x=x, mode=0, desc="262,144 independent 8x8 blocks of a 4096x4096 image "
                     "(U{0..255}-128, seed 1), forward DCT-II, contiguous (B,8,8)")
+    if name == "shapes":
+        return dict(x=None, mode=None, desc="every supported shape, 128 MiB batches of N(0,1) per shape, "
+                    "plain form, forward / inverse / round trip")
     if name == "image8":
         img = (np.random.default_rng(1).integers(0, 256, (4096, 4096)) - 128).astype(np.float32)
         return dict(x=img, mode=0, desc="4096x4096 image (U{0..255}-128, seed 1): its 262,144 8x8 blocks "
@@ -200,6 +203,10 @@ def run_reference_arm(args, rank: int, world: int):
     wl = workload(args.workload)
     x = wl["x"]
     threads = O.host_threads()
+    if x is None:
+        print(json.dumps({"impl": "reference", "unavailable": "the per-shape sweep has no reference arm; "
+                          "use the named workloads"}))
+        return
     if "items" in wl:
         return _reference_ragged(args, wl, world, threads)
     if x.ndim == 2:   # image workload: the reference needs the blocks copied out contiguously (untimed)
@@ -356,6 +363,8 @@ def main():
         return run_ragged(args, wl, rank, world, local, dist, torch)
     if args.workload == "image8":
         return run_image8(args, wl, rank, world, local, dist, torch)
+    if args.workload == "shapes":
+        return run_shapes(args, rank, local, torch)
     xh = wl["x"]
     if args.batch:
         xh = np.ascontiguousarray(np.resize(xh, (args.batch,) + xh.shape[1:]))
@@ -502,6 +511,10 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
     from oracle import oracle as O
 
     dev = torch.device("cuda", local)
+    if args.batch:   # the first N arrays of the mixed batch
+        items = wl["items"][:args.batch]
+        span = sum(h * w for h, w, _ in items)
+        wl = dict(wl, items=items, x=wl["x"][:span], desc=wl["desc"] + f"; first {len(items)} arrays")
     x = torch.from_numpy(wl["x"]).to(dev)
     tuning = None
     tfile = ROOT / "profiles" / "ragged_tuning.json"
@@ -570,6 +583,50 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
             "forms": out, "max_rel_err_output_scaled_sample": worst,
             "speedup_vs_launch_loop": out["launch_loop"]["ms_per_step"] / head["ms_per_step"],
             "clocks": head["clocks"], "gpu_launches": head["steps"]}))
+
+
+def run_shapes(args, rank, local, torch):
+    """Plain-form GB/s for all 64 shapes and three modes (device-resident, 128 MiB batches, two
+    rotating buffer sets = 256 MiB > L2, CUDA events over `steps` launches per mode)."""
+    from bridct_b200 import _lib, torch_api
+
+    lib = _lib.lib()
+    dev = torch.device("cuda", local)
+    sizes = [8, 16, 32, 64, 128, 256, 512, 1024]
+    pk = peaks()
+    table = {}
+    steps = max(3, min(args.steps, 50))
+    for h in sizes:
+        for w in sizes:
+            b = (128 << 20) // (h * w * 4)
+            gen = torch.Generator(device=dev).manual_seed(h * 4096 + w)
+            xs = [torch.randn(b, h, w, device=dev, generator=gen) for _ in range(2)]
+            ys = [torch.empty_like(xs[0]) for _ in range(2)]
+            plan = torch_api._plan(local, h, w)
+            row = []
+            for mode in range(3):
+                def launch(i):
+                    _lib.check(lib.bridct_plan_apply_device(plan, mode, xs[i % 2].data_ptr(), ys[i % 2].data_ptr(),
+                                                            b, None), "bridct_plan_apply_device")
+                for i in range(max(3, args.warmup)):
+                    launch(i)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for i in range(steps):
+                    launch(i)
+                e1.record()
+                torch.cuda.synchronize()
+                row.append(8.0 * b * h * w * steps / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+            table[f"{h}x{w}"] = {"arrays": b, "fwd": row[0], "inv": row[1], "rt": row[2],
+                                 "pct_hbm_fwd": 100 * row[0] / pk["hbm_gbs"]}
+            if rank == 0:
+                print(f"{h:5d}x{w:<5d} b={b:7d}  fwd {row[0]:6.0f}  inv {row[1]:6.0f}  rt {row[2]:6.0f} GB/s "
+                      f"({100 * row[0] / pk['hbm_gbs']:.1f}% HBM fwd)", file=sys.stderr, flush=True)
+            del xs, ys
+    if rank == 0:
+        print(json.dumps({"metric": "plain-form GB/s per shape (8 B per element)", "unit": "GB/s",
+                          "n_gpus": 1, "steps": steps, "peak_hbm_gbs": pk["hbm_gbs"], "shapes": table}))
 
 
 def run_image8(args, wl, rank, world, local, dist, torch):
