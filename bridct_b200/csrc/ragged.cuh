@@ -50,7 +50,7 @@ constexpr int kRaggedThreads = 192;                                 // 2 CTAs pe
 constexpr int kXbufPerWarp = cmax(cmax(FourStepSizes<4>::FLOATS, FourStepSizes<8>::FLOATS),
                                   cmax(FourStepSizes<16>::FLOATS, FourStepSizes<32>::FLOATS));
 constexpr int kRaggedXbuf = (kRaggedThreads / 32) * kXbufPerWarp;
-constexpr int kRaggedTile = 16384 + 1024;                           // worst-case tile floats (w+1 pitch)
+constexpr int kRaggedTile = 16384 + 1024;                           // worst-case tile floats (odd pitch)
 constexpr int kRaggedSmem = (kRaggedTile + kRaggedXbuf) * 4;
 constexpr unsigned kRaggedSpin = 1u << 22;                          // x ~256 ns back-off
 
@@ -87,25 +87,40 @@ __device__ __forceinline__ void lines_dyn(int n, int mode, float* tile, int nlin
 #undef BRIDCT_LINES_N
 }
 
+// Shared-memory pitch of a unit's block (rows x cols): aligned (cols + 4, float4 staging)
+// unless a column pass of 512- or 1024-point lines runs on it (their four-step groups put
+// every lane in one bank at an aligned pitch) or the aligned block would not fit the tile.
+__device__ __forceinline__ int ragged_pitch(int rows, int cols, bool column_pass, int h) {
+  if ((column_pass && h >= 512) || rows * (cols + 4) > kRaggedTile) return cols + 1;
+  return cols + 4;
+}
+
 // Loads rows x cols floats (row pitch gp in global) into shared memory (pitch P).
 __device__ __forceinline__ void load_block(const float* g, long long gp, int rows, int cols, float* s, int P,
                                            bool bypass_l1) {
   const int q = cols >> 2;
+  const bool vec = (P & 3) == 0;
   for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
     const int r = i / q, c = (i % q) * 4;
     const float4* p = reinterpret_cast<const float4*>(g + r * gp + c);
     const float4 v = bypass_l1 ? __ldcg(p) : __ldg(p);
     float* d = s + r * P + c;
-    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+    if (vec) {
+      *reinterpret_cast<float4*>(d) = v;
+    } else {
+      d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+    }
   }
 }
 
 __device__ __forceinline__ void store_block(float* g, long long gp, int rows, int cols, const float* s, int P) {
   const int q = cols >> 2;
+  const bool vec = (P & 3) == 0;
   for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
     const int r = i / q, c = (i % q) * 4;
     const float* v = s + r * P + c;
-    *reinterpret_cast<float4*>(g + r * gp + c) = make_float4(v[0], v[1], v[2], v[3]);
+    *reinterpret_cast<float4*>(g + r * gp + c) =
+        vec ? *reinterpret_cast<const float4*>(v) : make_float4(v[0], v[1], v[2], v[3]);
   }
 }
 
@@ -126,7 +141,7 @@ __global__ void __launch_bounds__(kRaggedThreads, 2) k_ragged(RaggedArgs a) {
     const float* xa = a.x + arr.offset;
     float* ya = a.y + arr.offset;
     if (unit.type == UNIT_TILE) {
-      const int P = w + 1;
+      const int P = ragged_pitch(h, w, true, h);
       load_block(xa, w, h, w, tile, P, false);
       __syncthreads();
       lines_dyn(h, mode, tile, w, P, StrideOff{1}, xbuf, pick_tables(a, h));
@@ -135,7 +150,7 @@ __global__ void __launch_bounds__(kRaggedThreads, 2) k_ragged(RaggedArgs a) {
       __syncthreads();
       store_block(ya, w, h, w, tile, P);
     } else if (unit.type == UNIT_COLSTRIP) {
-      const int tc = unit.count, P = tc + 1;
+      const int tc = unit.count, P = ragged_pitch(h, tc, true, h);
       load_block(xa + unit.first, w, h, tc, tile, P, false);
       __syncthreads();
       lines_dyn(h, mode, tile, tc, P, StrideOff{1}, xbuf, pick_tables(a, h));
@@ -160,7 +175,7 @@ __global__ void __launch_bounds__(kRaggedThreads, 2) k_ragged(RaggedArgs a) {
       }
       __syncthreads();
       if (s_ok) {
-        const int rb = unit.count, P = w + 1;
+        const int rb = unit.count, P = ragged_pitch(rb, w, false, 0);
         float* ga = ya + (long long)unit.first * w;
         load_block(ga, w, rb, w, tile, P, true);
         __syncthreads();
