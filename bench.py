@@ -608,7 +608,7 @@ def run_shapes(args, rank, local, torch):
                 def launch(i):
                     _lib.check(lib.bridct_plan_apply_device(plan, mode, xs[i % 2].data_ptr(), ys[i % 2].data_ptr(),
                                                             b, None), "bridct_plan_apply_device")
-                for i in range(max(3, args.warmup)):
+                for i in range(max(10, args.warmup)):
                     launch(i)
                 torch.cuda.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -39,6 +39,22 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
   using Gm = Geometry<H, W>;
   if (batch <= 0) return cudaSuccess;
   if constexpr (H == 8 && W == 8) {
+    // Measured on B200 (GB/s, device-resident, back-to-back launches): the double-buffered kernel
+    // wins forward/inverse batches up to a few hundred thousand arrays (262,144: 5131 vs 4937)
+    // and round trips from about 200,000 (524,288: 5655 vs 5130); the single-buffer kernel
+    // wins larger forward batches (1,048,576: 5930 vs 5355) and small round trips.
+    const bool db = MODE == LM_RT ? batch >= 196608 : batch <= 393216;
+    if (db) {
+      auto k = k_blocks8_db<MODE>;
+      constexpr int smem = 2 * kB8dbChunks * 16;
+      const int bps = kernel_blocks_per_sm(k, smem, kB8dbThreads);
+      if (bps <= 0) return cudaErrorInvalidConfiguration;
+      const long long ntiles = (batch + kB8dbThreads - 1) / kB8dbThreads;
+      long long grid = (long long)ctx.sm_count * bps;
+      if (grid > ntiles) grid = ntiles;
+      k<<<(unsigned)grid, kB8dbThreads, smem, st>>>(x, y, batch);
+      return cudaGetLastError();
+    }
     auto k = k_blocks8<MODE>;
     constexpr int smem = kB8Chunks * 16;
     const int bps = kernel_blocks_per_sm(k, smem, kB8Threads);

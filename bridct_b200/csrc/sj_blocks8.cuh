@@ -101,4 +101,83 @@ __global__ void __launch_bounds__(kB8Threads) k_blocks8(const float* __restrict_
   }
 }
 
+// Double-buffered variant: 128-array tiles (32 KB) in two shared-memory buffers filled with
+// cp.async, so each CTA has its next tile in flight while it transforms the current one (three
+// CTAs per SM).  Same work split: full rounds tile-strided, the last partial round spread over
+// all CTAs.
+constexpr int kB8dbThreads = 128;                  // arrays per tile = threads per CTA
+constexpr int kB8dbChunks = kB8dbThreads * 16;     // 16-byte chunks per tile
+
+__device__ __forceinline__ void b8_cp_async16(float4* dst, const float4* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kB8dbThreads) k_blocks8_db(const float* __restrict__ x, float* __restrict__ y,
+                                                             long long batch) {
+  extern __shared__ float4 s8[];
+  const long long round_arrays = (long long)gridDim.x * kB8dbThreads;
+  const long long full = batch / round_arrays;
+  const long long rest = batch - full * round_arrays;
+  const long long per = rest / gridDim.x, extra = rest % gridDim.x;
+  const long long nrounds = full + ((per + (blockIdx.x < extra ? 1 : 0)) > 0 ? 1 : 0);
+  const int t = threadIdx.x;
+  auto range = [&](long long round, long long& first, int& arrays) {
+    if (round < full) {
+      first = round * round_arrays + (long long)blockIdx.x * kB8dbThreads;
+      arrays = kB8dbThreads;
+    } else {
+      first = full * round_arrays + blockIdx.x * per + (blockIdx.x < extra ? blockIdx.x : extra);
+      arrays = (int)(per + (blockIdx.x < extra ? 1 : 0));
+    }
+  };
+  auto issue = [&](long long round) {
+    long long first;
+    int arrays;
+    range(round, first, arrays);
+    float4* buf = s8 + (round & 1) * kB8dbChunks;
+    const float4* src = reinterpret_cast<const float4*>(x) + first * 16;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int q = t + k * kB8dbThreads;
+      if (q < arrays * 16) b8_cp_async16(buf + b8_slot(q), src + q);
+    }
+  };
+  if (nrounds > 0) issue(0);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  for (long long round = 0; round < nrounds; ++round) {
+    if (round + 1 < nrounds) issue(round + 1);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 1;" ::: "memory");   // this round's copies have landed
+    __syncthreads();
+    long long first;
+    int arrays;
+    range(round, first, arrays);
+    float4* buf = s8 + (round & 1) * kB8dbChunks;
+    if (t < arrays) {
+      float v[64];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const float4 c = buf[b8_slot(t * 16 + j)];
+        v[4 * j] = c.x; v[4 * j + 1] = c.y; v[4 * j + 2] = c.z; v[4 * j + 3] = c.w;
+      }
+      b8_transform<MODE>(v);
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        buf[b8_slot(t * 16 + j)] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+    }
+    __syncthreads();
+    float4* dst = reinterpret_cast<float4*>(y) + first * 16;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int q = t + k * kB8dbThreads;
+      if (q < arrays * 16) dst[q] = buf[b8_slot(q)];
+    }
+    __syncthreads();   // the buffer is refilled by the next round's issue
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 }  // namespace bridct

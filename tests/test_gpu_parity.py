@@ -172,3 +172,20 @@ def test_linearity_and_orthogonality_full_size():
     np.testing.assert_allclose(ny, na, rtol=1e-6)
     back = gpu(ya, 1)
     assert err(back, a, a) <= TOL
+
+
+def test_blocks8_kernels_agree_bitwise():
+    # 8x8 batches run on one of two kernels chosen by batch size and mode (single-buffer tiles of
+    # 256 arrays, or double-buffered tiles of 128): the same register program, so the same bits.
+    import torch
+    from bridct_b200 import torch_api
+
+    big = torch.randn(400000, 8, 8, device="cuda")
+    head = big[:3000].clone()
+    for mode, n in ((0, 400000), (1, 400000), (2, 200000)):
+        y_big = torch_api.apply(big[:n], mode)
+        y_small = torch_api.apply(head, mode)
+        torch.cuda.synchronize()
+        assert torch.equal(y_big[:3000], y_small), mode
+        xs = head[:64].cpu().numpy()
+        assert O.rel_max_error(y_small[:64].cpu().numpy(), O.fp64_apply(xs, mode), xs, output_scaled=True) <= TOL
