@@ -80,11 +80,24 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
     for (long long b0 = 0; b0 < batch; b0 += chunk) {
       const long long nb = batch - b0 < chunk ? batch - b0 : chunk;
       const long long off = b0 * H * W;
-      TileArgs ac{x + off, y + off, nb * (W / Gm::kTC), nb * H, tab};
-      cudaError_t e = launch_tiles(kc, Gm::kSmemStrip, bpc, ac, ctx, st);
+      cudaError_t e;
+      if (nb * (W / Gm::kTC) < 2LL * ctx.sm_count) {   // few arrays: smaller strips and row blocks
+        auto kcs = k_colstrip<H, W, Gm::kTCs, MODE>;
+        TileArgs ac{x + off, y + off, nb * (W / Gm::kTCs), nb * H, tab};
+        e = launch_tiles(kcs, Gm::kSmemStripS, kernel_blocks_per_sm(kcs, Gm::kSmemStripS), ac, ctx, st);
+      } else {
+        TileArgs ac{x + off, y + off, nb * (W / Gm::kTC), nb * H, tab};
+        e = launch_tiles(kc, Gm::kSmemStrip, bpc, ac, ctx, st);
+      }
       if (e != cudaSuccess) return e;
-      TileArgs ar{y + off, y + off, nb * H / Gm::kRB, nb * H, tab};
-      e = launch_tiles(kr, Gm::kSmemRows, bpr, ar, ctx, st);
+      if (nb * H / Gm::kRB < 2LL * ctx.sm_count) {
+        auto krs = k_full<H, W, Gm::kRBs, false, true, MODE>;
+        TileArgs ar{y + off, y + off, nb * H / Gm::kRBs, nb * H, tab};
+        e = launch_tiles(krs, Gm::kSmemRowsS, kernel_blocks_per_sm(krs, Gm::kSmemRowsS), ar, ctx, st);
+      } else {
+        TileArgs ar{y + off, y + off, nb * H / Gm::kRB, nb * H, tab};
+        e = launch_tiles(kr, Gm::kSmemRows, bpr, ar, ctx, st);
+      }
       if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

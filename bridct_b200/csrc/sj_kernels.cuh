@@ -42,6 +42,7 @@ template <> struct ExchangeFloats<512> { static constexpr int value = FourStepSi
 template <> struct ExchangeFloats<1024> { static constexpr int value = FourStepSizes<32>::FLOATS; };
 
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int cmin(int a, int b) { return a < b ? a : b; }
 __host__ __device__ constexpr int round4(int a) { return (a + 3) & ~3; }
 
 // Floats of one line length's four-step tables in shared memory (post first: float4 aligned).
@@ -291,6 +292,12 @@ struct Geometry {
   }
   static constexpr int kRB = pick_rb();
   static constexpr int kSmemRows = rows_smem(kRB);
+  // Few-array variant: one four-step line group per warp, so that a call on one or a few arrays
+  // spreads over more SMs (a single 1024x1024 array: 128 strips instead of 64).
+  static constexpr int kTCs = H >= 128 ? cmin(kTC, cmax(4, kWarps * lines_per_warp<H>())) : kTC;
+  static constexpr int kSmemStripS = strip_smem(kTCs);
+  static constexpr int kRBs = W >= 128 ? cmin(kRB, kWarps * lines_per_warp<W>()) : kRB;
+  static constexpr int kSmemRowsS = rows_smem(kRBs);
 };
 
 }  // namespace bridct
