@@ -201,3 +201,32 @@ def test_two_pass_geometries_agree_bitwise(shape, big):
         y_one = torch_api.apply(x[:1].clone(), mode)
         torch.cuda.synchronize()
         assert torch.equal(y_batch[:1], y_one), (shape, mode)
+
+
+@pytest.mark.parametrize("n", [8, 16])
+def test_impulse_basis(n):
+    # every unit impulse of an n x n array (the reference's impulse-basis tests): each output is
+    # a column of the orthonormal 2D transform, so the outputs form an orthogonal matrix
+    x = np.zeros((n * n, n, n), np.float32)
+    x.reshape(n * n, n * n)[np.arange(n * n), np.arange(n * n)] = 1.0
+    for mode in range(3):
+        y = torch_api.apply(torch.from_numpy(x).cuda(), mode).cpu().numpy()
+        assert O.rel_max_error(y, O.fp64_apply(x, mode), x, output_scaled=True) <= TOL, mode
+        m = y.reshape(n * n, n * n).astype(np.float64)
+        assert np.abs(m @ m.T - np.eye(n * n)).max() <= 4 * TOL, mode
+
+
+@pytest.mark.parametrize("shape", [(8, 8), (32, 64), (256, 256), (1024, 128)])
+def test_constant_arrays_map_to_dc(shape):
+    # a constant array has only a DC coefficient c*sqrt(h*w) (the reference's DC tests)
+    h, w = shape
+    c = np.float32(-3.75)
+    x = np.full((2, h, w), c, np.float32)
+    y = torch_api.apply(torch.from_numpy(x).cuda(), 0).cpu().numpy()
+    dc = float(c) * np.sqrt(h * w)
+    assert np.abs(y[:, 0, 0] - dc).max() <= TOL * abs(dc)
+    rest = y.copy()
+    rest[:, 0, 0] = 0
+    assert np.abs(rest).max() <= TOL * abs(dc)
+    back = torch_api.apply(torch.from_numpy(y).cuda(), 1).cpu().numpy()
+    assert np.abs(back - c).max() <= TOL * abs(dc)
