@@ -332,17 +332,20 @@ __device__ __forceinline__ void issue_mmas(uint32_t sstage, uint32_t sabuf, uint
   }
 }
 
-// Warp roles of k_tc8 (12 warps):
+// Warp roles of k_tc8 (16 warps):
 //   warp 0 lane 0  TMA producer: ring tile s <- X tile j      (waits stage_free, arms stage_full)
 //                  (ring depth: 5 tiles for BF16x3, 4 for TF32x3)
 //   warp 1 lane 0  MMA issuer: TMEM acc t <- A buffer a . B    (waits a_full, acc_free;
 //                  commits to acc_full and a_free)
 //   warp 2         TMEM allocator / deallocator
-//   warps 4-7      split: ring tile s -> A buffer a            (waits stage_full, a_free)
-//   warps 8-11     epilogue: acc t -> registers -> ring tile s -> TMA store
+//   warps 4-7      split group 0: even tiles, ring tile s -> A buffer 0  (waits stage_full, a_free)
+//   warps 8-11     split group 1: odd tiles, ring tile s -> A buffer 1
+//   warps 12-15    epilogue: acc t -> ring tile s (16 columns at a time) -> TMA store
 //                  (waits acc_full; frees acc t, then ring tile s once the store has read it)
-// Tile j of this CTA uses ring tile j % kStages, A buffer j % 2 and accumulator j % 2.
-constexpr int kWsThreads = 384;
+// Tile j of this CTA uses ring tile j % kStages, A buffer j % 2 and accumulator j % 2.  The split
+// is the longest role per tile, so two groups (one warp per sub-partition each) alternate.
+constexpr int kWsThreads = 384;     // the pass kernels' role layout
+constexpr int kTc8Threads = 512;
 
 struct Bars {
   uint32_t stage_full, stage_free, a_full, a_free, acc_full, acc_free;
@@ -355,7 +358,7 @@ struct Bars {
 // x, y: tensor maps of the (batch x 64) FP32 matrices (box 32 x 128, SWIZZLE_128B).
 // bimage: the B operand shared-memory image (Layout<FORM>::kBImage bytes, 16-byte aligned).
 template <int FORM>
-__global__ void __launch_bounds__(kWsThreads, 1) k_tc8(const __grid_constant__ CUtensorMap xmap,
+__global__ void __launch_bounds__(kTc8Threads, 1) k_tc8(const __grid_constant__ CUtensorMap xmap,
                                                         const __grid_constant__ CUtensorMap ymap,
                                                         const uint4* __restrict__ bimage, int ntiles,
                                                         int* __restrict__ err) {
@@ -367,7 +370,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_tc8(const __grid_constant__ C
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + L::kBarOff + L::kTmemSlot);
   constexpr int kStages = L::kStages;
   __shared__ volatile int s_abort;
-  __shared__ volatile int s_group_ok[2];
+  __shared__ volatile int s_group_ok[3];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ntile_local = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
@@ -394,7 +397,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_tc8(const __grid_constant__ C
   }
   {
     uint4* dst = reinterpret_cast<uint4*>(base + L::kBOff);
-    for (int i = tid; i < L::kBImage / 16; i += kWsThreads) dst[i] = __ldg(bimage + i);
+    for (int i = tid; i < L::kBImage / 16; i += kTc8Threads) dst[i] = __ldg(bimage + i);
   }
   fence_async_smem();
   tc_fence_before();
@@ -431,29 +434,32 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_tc8(const __grid_constant__ C
       const int j = ntile_local - 1;
       ok = mbar_wait(bars.a_free + 8 * (j % kABufs), (uint32_t)(j / kABufs) & 1u);
     }
-  } else if (warp >= 4 && warp < 8) {
-    // Only the group leader polls the mbarriers (bounded) and broadcasts the outcome, so the
-    // group's named barrier is reached by all 128 threads whatever the outcome.
-    const uint32_t r = tid - 128;
-    for (int j = 0; j < ntile_local; ++j) {
+  } else if (warp >= 4 && warp < 12) {
+    // Two split groups alternate tiles; in each, only the leader polls the mbarriers (bounded)
+    // and broadcasts the outcome, so the group's named barrier is reached by all 128 threads
+    // whatever the outcome.
+    const int grp = (warp - 4) >> 2;            // 0: even tiles, 1: odd tiles
+    const uint32_t r = tid - 128 - 128 * grp;
+    const int bar_id = grp ? 3 : 1, ok_slot = grp ? 2 : 0;
+    for (int j = grp; j < ntile_local; j += 2) {
       const int s = j % kStages, a = j % kABufs;
       if (r == 0) {
         bool g = !s_abort && mbar_wait(bars.stage_full + 8 * s, (uint32_t)(j / kStages) & 1u);
         if (g) g = mbar_wait(bars.a_free + 8 * a, ((uint32_t)(j / kABufs) & 1u) ^ 1u);
-        s_group_ok[0] = g ? 1 : 0;
+        s_group_ok[ok_slot] = g ? 1 : 0;
       }
-      named_sync(1, 128);
-      if (!s_group_ok[0]) {
+      named_sync(bar_id, 128);
+      if (!s_group_ok[ok_slot]) {
         ok = r != 0;      // the leader reports the expiry
         break;
       }
       split_tile<FORM>(base + L::kStageOff + s * kTile, base + L::kAOff + a * Sizes<FORM>::kABuf, r);
       fence_async_smem();
-      named_sync(1, 128);
+      named_sync(bar_id, 128);
       if (r == 0) mbar_arrive(bars.a_full + 8 * a);
     }
-  } else if (warp >= 8) {
-    const uint32_t r = tid - 256;               // tile row = TMEM lane
+  } else if (warp >= 12) {
+    const uint32_t r = tid - 384;               // tile row = TMEM lane
     const uint32_t quarter = (uint32_t)(warp & 3) * 32u;
     for (int j = 0; j < ntile_local; ++j) {
       const int s = j % kStages, t = j % kAccs;
@@ -464,8 +470,9 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_tc8(const __grid_constant__ C
         break;
       }
       tc_fence_after();
-      float v[64];
+      // the MMAs that read ring tile s are complete (acc_full), so the result goes straight into it
       const uint32_t taddr = tmem_base + t * kTmemCols + (quarter << 16);
+      uint8_t* out = base + L::kStageOff + s * kTile;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         float big[16], sm[16];
@@ -481,21 +488,19 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_tc8(const __grid_constant__ C
           tmem_wait_ld();
         }
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[q * 16 + i] = big[i] + sm[i];
+        for (int c4 = 0; c4 < 4; ++c4) {
+          const int col = q * 16 + c4 * 4;
+          const uint32_t off = (col >> 5) * 16384u + sw128(r, (col & 31) >> 2);
+          *reinterpret_cast<float4*>(out + off) =
+              make_float4(big[4 * c4] + sm[4 * c4], big[4 * c4 + 1] + sm[4 * c4 + 1],
+                          big[4 * c4 + 2] + sm[4 * c4 + 2], big[4 * c4 + 3] + sm[4 * c4 + 3]);
+        }
       }
       tc_fence_before();
-      named_sync(2, 128);
-      if (r == 0) mbar_arrive(bars.acc_free + 8 * t);
-      uint8_t* out = base + L::kStageOff + s * kTile;
-#pragma unroll
-      for (int c = 0; c < 16; ++c) {
-        const int col = c * 4;
-        const uint32_t off = (col >> 5) * 16384u + sw128(r, (col & 31) >> 2);
-        *reinterpret_cast<float4*>(out + off) = make_float4(v[col], v[col + 1], v[col + 2], v[col + 3]);
-      }
       fence_async_smem();
       named_sync(2, 128);
       if (r == 0) {
+        mbar_arrive(bars.acc_free + 8 * t);
         const int tile = blockIdx.x + j * gridDim.x;
         tma_store_2d(&ymap, 0, tile * kRows, sbase + L::kStageOff + s * kTile);
         tma_store_2d(&ymap, 32, tile * kRows, sbase + L::kStageOff + s * kTile + 16384u);

@@ -539,7 +539,7 @@ int launch_tc8(const bridct_plan* p, int inverse, const float* x, float* y, size
                TcDevice* d) {
   using L = tc::Layout<FORM>;
   auto k = tc::k_tc8<FORM>;
-  const int bps = kernel_setup(reinterpret_cast<const void*>(k), L::kDynamic, tc::kWsThreads);
+  const int bps = kernel_setup(reinterpret_cast<const void*>(k), L::kDynamic, tc::kTc8Threads);
   if (bps <= 0) return cuda_fail(cudaErrorInvalidConfiguration, "k_tc8 occupancy");
   CUtensorMap xm, ym;
   if (!make_map(&xm, x, batch) || !make_map(&ym, y, batch)) {
@@ -549,7 +549,7 @@ int launch_tc8(const bridct_plan* p, int inverse, const float* x, float* y, size
   const int ntiles = (int)((batch + tc::kRows - 1) / tc::kRows);
   int grid = p->dev->sm_count * bps;
   if (grid > ntiles) grid = ntiles;
-  k<<<grid, tc::kWsThreads, L::kDynamic, st>>>(xm, ym, reinterpret_cast<const uint4*>(d->images[FORM][inverse]),
+  k<<<grid, tc::kTc8Threads, L::kDynamic, st>>>(xm, ym, reinterpret_cast<const uint4*>(d->images[FORM][inverse]),
                                                ntiles, d->err);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_tc8 launch");
