@@ -344,7 +344,6 @@ __device__ __forceinline__ void issue_mmas(uint32_t sstage, uint32_t sabuf, uint
 //                  (waits acc_full; frees acc t, then ring tile s once the store has read it)
 // Tile j of this CTA uses ring tile j % kStages, A buffer j % 2 and accumulator j % 2.  The split
 // is the longest role per tile, so two groups (one warp per sub-partition each) alternate.
-constexpr int kWsThreads = 384;     // the pass kernels' role layout
 constexpr int kTc8Threads = 512;
 
 struct Bars {

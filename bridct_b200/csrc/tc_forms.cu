@@ -294,7 +294,7 @@ int launch_pass(const bridct_plan* p, bool inverse, const float* x, float* out, 
                 cudaStream_t st, TcDevice* d) {
   using PL = tc::PassLayout<FORM, L>;
   auto k = tc::k_tcpass<FORM, L>;
-  if (kernel_setup(reinterpret_cast<const void*>(k), PL::kDynamic, tc::kWsThreads) <= 0)
+  if (kernel_setup(reinterpret_cast<const void*>(k), PL::kDynamic, tc::kPassThreads) <= 0)
     return cuda_fail(cudaErrorInvalidConfiguration, "k_tcpass shared memory");
   const uint4* img = pass_image_device<FORM, L>(d, inverse);
   if (!img) return cuda_fail(cudaGetLastError(), "tensor-core coefficient upload");
@@ -307,7 +307,7 @@ int launch_pass(const bridct_plan* p, bool inverse, const float* x, float* out, 
   long long slots = p->dev->sm_count / PL::kBlocks;
   if (slots > mtiles) slots = mtiles;
   if (slots < 1) slots = 1;
-  k<<<(unsigned)(slots * PL::kBlocks), tc::kWsThreads, PL::kDynamic, st>>>(xm, out, img, (long long)rows, rshift,
+  k<<<(unsigned)(slots * PL::kBlocks), tc::kPassThreads, PL::kDynamic, st>>>(xm, out, img, (long long)rows, rshift,
                                                                          d->err);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_tcpass launch");

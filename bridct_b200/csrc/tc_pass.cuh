@@ -16,13 +16,15 @@
 // Split precision as in the 8x8 forms: BF16x3 = six products of 3-way splits, TF32x3 = three
 // products of 2-way splits, all accumulated in FP32 in TMEM.
 //
-// Warp roles (384 threads):
+// Warp roles (512 threads):
 //   warp 0 lane 0  TMA producer: ring stage s <- K-chunk of an M-tile (waits stage_free)
 //   warp 1 lane 0  MMA issuer: TMEM acc set t += splits(stage s, A buffer a) . B slice; commits
 //                  stage_free/a_free per chunk and acc_full after an M-tile's last chunk
 //   warp 2         TMEM allocator
-//   warps 4-7      split: stage s (FP32) -> hi/mid in place + lo into A buffer a
-//   warps 8-11     epilogue: sum of acc set t -> registers (frees set t) -> transposed stores
+//   warps 4-7      split group 0 (even K-chunks), warps 8-11 split group 1 (odd K-chunks):
+//                  stage s (FP32) -> hi/mid in place + lo into A buffer j % 2
+//   warps 12-15    epilogue: sum of acc set t, 16 columns at a time -> transposed stores,
+//                  then frees set t
 // Every wait is bounded; on expiry the CTA sets *err and all roles leave their loops.
 #pragma once
 #include "tc_blocks8.cuh"
@@ -48,6 +50,7 @@ constexpr int kBAtom = 64 * 128;         // one K-major SW128 atom column of 64 
 constexpr int kPassNBlock = 64;          // output columns per CTA (MMA N)
 constexpr int kPassSmemMax = 232448;     // opt-in shared memory per block
 constexpr int kPassMaxStages = 6;
+constexpr int kPassThreads = 512;
 
 constexpr int pass_min(int a, int b) { return a < b ? a : b; }
 
@@ -158,7 +161,7 @@ __device__ __forceinline__ void issue_pass_mmas(uint32_t sstage, uint32_t sabuf,
 // the transposed arrays (R rows per array, rshift = log2 R).  bimage: kBlocks slices of
 // PassLayout::kBBytes.  Grid: a multiple of kBlocks CTAs; CTA c computes N-block c % kBlocks.
 template <int FORM, int L>
-__global__ void __launch_bounds__(kWsThreads, 1)
+__global__ void __launch_bounds__(kPassThreads, 1)
     k_tcpass(const __grid_constant__ CUtensorMap xmap, float* __restrict__ out,
              const uint4* __restrict__ bimage, long long nrows, int rshift, int* __restrict__ err) {
   using PL = PassLayout<FORM, L>;
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   const PassBars bars(sbase + PL::kBarOff);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + PL::kBarOff + 16 * kPassMaxStages + 64);
   __shared__ volatile int s_abort;
-  __shared__ volatile int s_group_ok[2];
+  __shared__ volatile int s_group_ok[3];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   const int nblk = blockIdx.x % PL::kBlocks;
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   {
     const uint4* src = bimage + (size_t)nblk * (PL::kBBytes / 16);
     uint4* dst = reinterpret_cast<uint4*>(base + PL::kBOff);
-    for (int i = tid; i < PL::kBBytes / 16; i += kWsThreads) dst[i] = __ldg(src + i);
+    for (int i = tid; i < PL::kBBytes / 16; i += kPassThreads) dst[i] = __ldg(src + i);
   }
   fence_async_smem();
   tc_fence_before();
@@ -246,17 +249,19 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       const long long j = nchunk_local - 1;
       ok = mbar_wait(bars.a_free + 8 * (int)(j & 1), (uint32_t)(j >> 1) & 1u);
     }
-  } else if (warp >= 4 && warp < 8) {
-    const uint32_t r = tid - 128;
-    for (long long j = 0; j < nchunk_local; ++j) {
+  } else if (warp >= 4 && warp < 12) {
+    const int grp = (warp - 4) >> 2;              // 0: even K-chunks, 1: odd K-chunks
+    const uint32_t r = tid - 128 - 128 * grp;
+    const int bar_id = grp ? 3 : 1, ok_slot = grp ? 2 : 0;
+    for (long long j = grp; j < nchunk_local; j += 2) {
       const int s = (int)(j % kStages), a = (int)(j & 1);
       if (r == 0) {
         bool g = !s_abort && mbar_wait(bars.stage_full + 8 * s, (uint32_t)(j / kStages) & 1u);
         if (g) g = mbar_wait(bars.a_free + 8 * a, ((uint32_t)(j >> 1) & 1u) ^ 1u);
-        s_group_ok[0] = g ? 1 : 0;
+        s_group_ok[ok_slot] = g ? 1 : 0;
       }
-      named_sync(1, 128);
-      if (!s_group_ok[0]) {
+      named_sync(bar_id, 128);
+      if (!s_group_ok[ok_slot]) {
         ok = r != 0;
         break;
       }
@@ -265,11 +270,11 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       if constexpr (FORM == BF16X3) split_tile<BF16X3>(stage, abuf, r);
       else split_box_tf32(stage, abuf, r);
       fence_async_smem();
-      named_sync(1, 128);
+      named_sync(bar_id, 128);
       if (r == 0) mbar_arrive(bars.a_full + 8 * a);
     }
-  } else if (warp >= 8) {
-    const uint32_t r = tid - 256;                 // tile row = TMEM lane
+  } else if (warp >= 12) {
+    const uint32_t r = tid - 384;                 // tile row = TMEM lane
     const uint32_t quarter = (uint32_t)(warp & 3) * 32u;
     const long long rmask = (1ll << rshift) - 1;
     for (long long jt = 0; jt < ntile_local; ++jt) {
@@ -282,7 +287,11 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         break;
       }
       tc_fence_after();
-      float v[kPassNBlock];
+      // row g = (array b, row h of that array); its column n goes to out[b][n][h]
+      const long long g = (slot + jt * nslots) * kRows + r;
+      const bool live = g < nrows;
+      const long long b = g >> rshift, h = g & rmask;
+      float* dst = out + ((b * L + (long long)nblk * kPassNBlock) << rshift) + h;
       const uint32_t taddr = tmem_base + t * kTileCols + (quarter << 16);
 #pragma unroll
       for (int q = 0; q < kPassNBlock / 16; ++q) {
@@ -304,20 +313,14 @@ __global__ void __launch_bounds__(kWsThreads, 1)
 #pragma unroll
           for (int i = 0; i < 16; ++i) big[i] += w[i];
         }
+        if (live) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[q * 16 + i] = big[i] + sm[i];
+          for (int i = 0; i < 16; ++i) dst[(long long)(q * 16 + i) << rshift] = big[i] + sm[i];
+        }
       }
       tc_fence_before();
       named_sync(2, 128);
       if (r == 0) mbar_arrive(bars.acc_free + 8 * t);
-      // row g = (array b, row h of that array); its column n goes to out[b][n][h]
-      const long long g = (slot + jt * nslots) * kRows + r;
-      if (g < nrows) {
-        const long long b = g >> rshift, h = g & rmask;
-        float* dst = out + ((b * L + (long long)nblk * kPassNBlock) << rshift) + h;
-#pragma unroll
-        for (int c = 0; c < kPassNBlock; ++c) dst[(long long)c << rshift] = v[c];
-      }
     }
   }
   if (!ok) {
