@@ -44,7 +44,7 @@ struct RaggedArgs {
   FourStepTables tab[4];    // N = 128, 256, 512, 1024
 };
 
-constexpr int kRaggedThreads = 192;                                 // 2 CTAs per SM at <= 168 registers
+constexpr int kRaggedThreads = 256;                                 // 2 CTAs per SM at <= 128 registers
 // Exchange floats per warp, worst case over the four-step widths G = 4..32 (G = 4 needs most:
 // 8 lines x 17 columns x pitch 5 x re/im).
 constexpr int kXbufPerWarp = cmax(cmax(FourStepSizes<4>::FLOATS, FourStepSizes<8>::FLOATS),
