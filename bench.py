@@ -8,9 +8,11 @@ Default workload: 262,144 independent 8x8 blocks of a 4096x4096 image (pixels un
 0..255 minus 128, seed 1), forward DCT-II, blocks stored contiguously as (B, 8, 8).  A step is
 one forward transform of all blocks (one pass of the hot path over the batch).  Algorithmic
 traffic is 8 bytes per element (read 4, write 4).  Timed steps replay a CUDA graph of
-launches over 4 rotating input/output buffer sets (512 MiB, larger than the 126 MB L2), timed
-with CUDA events on the launching stream; multi-GPU runs are independent replicas per GPU
-(the batch shards with no exchange step), timed as the max over ranks.
+launches over rotating input/output buffer sets that together exceed the 126 MB L2 (two sets,
+256 MiB, on the default workload), timed with CUDA events on the launching stream; multi-GPU
+runs are independent replicas per GPU (the batch shards with no exchange step), timed as the
+max over ranks.  Tensor-core forms also report their FLOP rate against the measured tensor
+peak; the CPU baseline reports all host threads and one thread.
 
 `e2e` is the same metric through the public C-ABI (bridct_plan_apply_batch) from pinned host
 buffers: every step copies the inputs host->device and the results device->host.
@@ -193,6 +195,45 @@ def cpu_reference(x: np.ndarray, mode: int, threads: int, budget_s: float):
     t = _ref_call(x, mode, n, threads, reps)
     gbs = 8.0 * h * w * n * reps / t / 1e9
     return gbs, f"{n} of {b} arrays x {reps} passes ({t:.2f} s, {threads} threads, one plan per thread)"
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_single_thread(x: np.ndarray, mode: int, budget_s: float = 0.5):
+    """The reference library on one host thread (GB/s) over a bounded sample."""
+    from oracle import oracle as O
+
+    if not O.bench_available():
+        return None
+    b, h, w = x.shape
+    n = ref_sample_size(x, mode, 1, 0.1)
+    t1 = _ref_call(x, mode, n, 1, 1)
+    reps = max(1, int(budget_s / max(t1, 1e-9)))
+    return 8.0 * h * w * n * reps / _ref_call(x, mode, n, 1, reps) / 1e9
+
+
+def tensor_rate(form: str, h: int, w: int, elems_per_s: float, pk: dict):
+    """Tensor-core FLOP rate of a form: 2*h*w*P flop per element for the 8x8 Kronecker GEMM,
+    2*(h+w)*P for the two separable passes (P = products: 6 BF16x3, 3 TF32x3, 1 FP8 plus its
+    refinement's second FP8 transform), against the measured bf16 peak (TF32 runs at half the
+    bf16 rate and FP8 at twice, nominally)."""
+    prods = {"tc_bf16x3": 6, "tc_tf32x3": 3, "tc_fp8": 2}.get(form)
+    if prods is None:
+        return None
+    per_elem = 2.0 * h * w * prods if (h, w) == (8, 8) else 2.0 * (h + w) * prods
+    tflops = per_elem * elems_per_s / 1e12
+    scale = {"tc_bf16x3": 1.0, "tc_tf32x3": 0.5, "tc_fp8": 2.0}[form]
+    peak = pk["bf16_tflops"] * scale
+    return {"tflops": tflops, "peak_tflops": peak, "frac": tflops / peak,
+            "peak_source": f"{pk['source']} bf16 burst x {scale}"}
 
 
 def run_reference_arm(args, rank: int, world: int):
@@ -466,7 +507,8 @@ def main():
         threads = O.host_threads()
         gbs, sample_txt = cpu_reference(xh, mode, threads, budget_s=2.0)
         if gbs is not None:
-            cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "reference", "sample": sample_txt}
+            cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "reference", "sample": sample_txt,
+                   "cpu_model": cpu_model(), "single_thread_gbs": cpu_single_thread(xh, mode)}
 
     if world > 1:
         dist.barrier()
@@ -495,7 +537,9 @@ def main():
                      "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"],
                      "traffic": traffic, "algorithmic_bytes_per_launch": bytes_step},
         "forms": {n: {**results[n], "gbs": timings[n]["gbs"], "ms_per_step": timings[n]["ms_per_step"],
-                      "pct_hbm": 100 * timings[n]["gbs"] / world / pk["hbm_gbs"]} for n in timings},
+                      "pct_hbm": 100 * timings[n]["gbs"] / world / pk["hbm_gbs"],
+                      "tensor": tensor_rate(n, h, w, b * h * w / (timings[n]["ms_per_step"] * 1e-3), pk)}
+                  for n in timings},
         "clocks": timings[head]["clocks"],
         "e2e": e2e,
         "gpu_launches": int(args.steps * launches_per_step(h, w, b)),
