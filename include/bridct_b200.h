@@ -16,10 +16,12 @@ extern "C" {
 
 /* Execution form of a transform. */
 enum bridct_form {
-    BRIDCT_FORM_SJ = 0,        /* FP32 Shao-Johnson CUDA-core kernels (the plan API's form) */
-    BRIDCT_FORM_TC_BF16X3 = 1, /* tensor cores: 3-term bf16 split of X, 6 products, FP32 acc. */
-    BRIDCT_FORM_TC_TF32X3 = 2, /* tensor cores: 2-term tf32 split of X and C, 3 products     */
-    BRIDCT_FORM_TC_FP8 = 3     /* FP8 E4M3, per-32x32-tile scale, + one FP32 refinement step */
+    BRIDCT_FORM_SJ = 0,        /* FP32 Shao-Johnson CUDA-core kernels (the plan API's form); all shapes */
+    BRIDCT_FORM_TC_BF16X3 = 1, /* tensor cores: 3-term bf16 split of X, 6 products, FP32 accumulation;
+                                  8x8 arrays, and arrays whose axes are 64, 128 or 256 */
+    BRIDCT_FORM_TC_TF32X3 = 2, /* tensor cores: 2-term tf32 split of X and C, 3 products; same shapes */
+    BRIDCT_FORM_TC_FP8 = 3     /* FP8 E4M3, per-32x32-tile scales, + one FP32 refinement step;
+                                  arrays whose axes are 128 or 256 */
 };
 
 /* Thread-local description of the last failure in this thread ("" if none). */
@@ -44,7 +46,10 @@ BRIDCT_API int bridct_plan_apply_device(bridct_plan *plan, enum bridct_mode mode
                                         void *stream);
 
 /* As bridct_plan_apply_device, with an explicit execution form (precision forms run
- * on the tensor cores; see enum bridct_form for the shapes each form supports). */
+ * on the tensor cores; see enum bridct_form for the shapes each form supports).  The
+ * tensor-core forms on axes of 64..256 and the FP8 form keep their intermediate in scratch
+ * owned by the plan (allocated by the first call that needs it, so make that call before any
+ * stream capture): calls on one plan must not run concurrently on different streams. */
 BRIDCT_API int bridct_plan_apply_form_device(bridct_plan *plan, enum bridct_mode mode,
                                              enum bridct_form form, const float *input,
                                              float *output, size_t batch, void *stream);
