@@ -465,7 +465,7 @@ def emit_function(g: Graph, name: str, in_names: Sequence[str], outputs: Sequenc
 # The generated set
 # ----------------------------------------------------------------------------------------
 
-REG_SIZES = (8, 16, 32, 64)         # whole line in one thread's registers
+REG_SIZES = (8, 16, 32, 64, 128)    # whole line in one thread's registers
 LEAF = 32                           # four-step leaf length for N >= 128
 STAGE2_SIZES = (4, 8, 16, 32)       # G = N / LEAF
 

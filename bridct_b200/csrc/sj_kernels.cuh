@@ -21,6 +21,14 @@ namespace bridct {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kTileFloats = 8192;   // target floats per CTA tile for small arrays
+// Longest line run as one thread's straight-line program for a pass of N-point lines whose
+// array has `other` points on the other axis.  128-point register lines (168 registers, no
+// spills) measured +12-59% over the four-step on 128x128, the two-pass shapes and forward /
+// inverse tiles with a short other axis, and -6..-28% on round trips of tiles with a short
+// other axis and on tiles mixing them with 64-point lines: those keep the four-step.
+__host__ __device__ constexpr int reg_line_max(int N, int other, int mode, bool two_pass) {
+  return N == 128 && (two_pass || other >= 128 || (mode != LM_RT && other <= 32)) ? 128 : 64;
+}
 
 struct LineTables {
   FourStepTables col;   // for line length h (used when h >= 128)
@@ -146,11 +154,12 @@ __device__ __forceinline__ void tile_store(float* g, long long gp, int rows, int
 }
 
 // Runs all lines of length N in a set of `nlines` lines; line l starts at tile + off(l),
-// elements at stride es.  Register lines for N <= 64, warp four-step lines above.
-template <int N, int MODE, typename Off>
+// elements at stride es.  Register lines (one thread per line) for N <= REG_MAX, warp
+// four-step lines above.
+template <int N, int MODE, int REG_MAX = 64, typename Off>
 __device__ __forceinline__ void run_lines(float* tile, int nlines, int es, const Off& off,
                                           float* xbuf, FourStepTables tab) {
-  if constexpr (N <= 64) {
+  if constexpr (N <= REG_MAX) {
     for (int l = threadIdx.x; l < nlines; l += blockDim.x) reg_line<N, MODE>(tile + off(l), es);
   } else {
     constexpr int G = N / 32;
@@ -201,12 +210,12 @@ __global__ void __launch_bounds__(kThreads) k_full(TileArgs a) {
     }
     if constexpr (DO_COL) {
       static_assert(TR % H == 0, "column pass needs whole arrays");
-      run_lines<H, MODE>(tile, (TR / H) * W, P,
+      run_lines<H, MODE, reg_line_max(H, W, MODE, false)>(tile, (TR / H) * W, P,
                          [](int l) { return (l / W) * H * P + (l % W); }, xbuf, tcol);
       __syncthreads();
     }
     if constexpr (DO_ROW) {
-      run_lines<W, MODE>(tile, TR, 1, [](int l) { return l * P; }, xbuf, trow);
+      run_lines<W, MODE, reg_line_max(W, H, MODE, !DO_COL)>(tile, TR, 1, [](int l) { return l * P; }, xbuf, trow);
       __syncthreads();
     }
     tile_store<P>(a.y + t * (long long)TR * W, W, rows, W, tile);
@@ -240,7 +249,7 @@ __global__ void __launch_bounds__(kThreads) k_colstrip(TileArgs a) {
       tile_load<P>(a.x + arr * (long long)H * W + s * TC, W, H, TC, tile, H);
       __syncthreads();
     }
-    run_lines<H, MODE>(tile, TC, P, [](int l) { return l; }, xbuf, tcol);
+    run_lines<H, MODE, reg_line_max(H, W, MODE, true)>(tile, TC, P, [](int l) { return l; }, xbuf, tcol);
     __syncthreads();
     tile_store<P>(a.y + arr * (long long)H * W + s * TC, W, H, TC, tile);
     __syncthreads();

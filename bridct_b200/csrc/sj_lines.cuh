@@ -31,7 +31,8 @@ namespace bridct {
 enum LineMode { LM_FWD = 0, LM_INV = 1, LM_RT = 2 };
 
 // ---------------------------------------------------------------------------------------
-// Register lines (N <= 64)
+// Register lines (N <= 128; the fixed-shape kernels use them for N = 128, the ragged kernel
+// only up to 64)
 // ---------------------------------------------------------------------------------------
 template <int N> struct RegLine;
 #define BRIDCT_REGLINE(N)                                                                  \
@@ -44,6 +45,7 @@ BRIDCT_REGLINE(8)
 BRIDCT_REGLINE(16)
 BRIDCT_REGLINE(32)
 BRIDCT_REGLINE(64)
+BRIDCT_REGLINE(128)
 #undef BRIDCT_REGLINE
 
 template <int N, int MODE>
