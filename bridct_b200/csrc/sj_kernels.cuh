@@ -82,6 +82,13 @@ __device__ __forceinline__ FourStepTables stage_tables(FourStepTables g, float* 
 // four-step lines with G >= 16 (h >= 512), whose stage-1 reads need an odd pitch (w + 1).
 __host__ __device__ constexpr bool odd_pitch(int h, bool has_col) { return has_col && h >= 512; }
 __host__ __device__ constexpr int pitch_of(int h, int w, bool has_col) { return odd_pitch(h, has_col) ? w + 1 : w + 4; }
+// Pitches of the two-pass kernels, whose long lines all run the four-step.  Chosen with a bank
+// model of the four-step's shared-memory accesses (Makhoul gather, post-rotation stores, exchange):
+// a column strip of 256-point lines with pitch tc + 2 (= 2 mod 4) and row blocks of 256- and
+// 512-point lines with pitch w + 8 (= 8 mod 32) and w + 16 (= 16 mod 32) need 20%, 23% and 14%
+// fewer wavefronts per line than with pitch + 4; tc + 2 rows are staged with 64-bit accesses.
+__host__ __device__ constexpr int strip_pitch(int h, int tc) { return h == 256 ? tc + 2 : pitch_of(h, tc, true); }
+__host__ __device__ constexpr int rowblock_pitch(int w) { return w == 256 ? w + 8 : w == 512 ? w + 16 : w + 4; }
 
 // Moves rows x cols floats between global memory (row pitch gp) and the tile (pitch P).
 template <int P>
@@ -95,6 +102,9 @@ __device__ __forceinline__ void tile_load(const float* g, long long gp, int rows
     float* d = tile + r * P + c;
     if constexpr (P % 4 == 0) {
       *reinterpret_cast<float4*>(d) = v;
+    } else if constexpr (P % 2 == 0) {
+      reinterpret_cast<float2*>(d)[0] = make_float2(v.x, v.y);
+      reinterpret_cast<float2*>(d)[1] = make_float2(v.z, v.w);
     } else {
       d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
     }
@@ -129,6 +139,9 @@ struct TileRegs {
         float* d = tile + r * P + c;
         if constexpr (P % 4 == 0) {
           *reinterpret_cast<float4*>(d) = v[k];
+        } else if constexpr (P % 2 == 0) {
+          reinterpret_cast<float2*>(d)[0] = make_float2(v[k].x, v[k].y);
+          reinterpret_cast<float2*>(d)[1] = make_float2(v[k].z, v[k].w);
         } else {
           d[0] = v[k].x; d[1] = v[k].y; d[2] = v[k].z; d[3] = v[k].w;
         }
@@ -146,6 +159,9 @@ __device__ __forceinline__ void tile_store(float* g, long long gp, int rows, int
     float4 v;
     if constexpr (P % 4 == 0) {
       v = *reinterpret_cast<const float4*>(sp);
+    } else if constexpr (P % 2 == 0) {
+      const float2 lo = reinterpret_cast<const float2*>(sp)[0], hi = reinterpret_cast<const float2*>(sp)[1];
+      v = make_float4(lo.x, lo.y, hi.x, hi.y);
     } else {
       v = make_float4(sp[0], sp[1], sp[2], sp[3]);
     }
@@ -177,7 +193,7 @@ __device__ __forceinline__ void run_lines(float* tile, int nlines, int es, const
 // matrix.  With DO_COL the tile holds TR/H whole arrays.
 template <int H, int W, int TR, bool DO_COL, bool DO_ROW, int MODE>
 __global__ void __launch_bounds__(kThreads) k_full(TileArgs a) {
-  constexpr int P = pitch_of(H, W, DO_COL);
+  constexpr int P = DO_COL ? pitch_of(H, W, true) : rowblock_pitch(W);
   constexpr int XB = kWarps * cmax(DO_COL ? ExchangeFloats<H>::value : 0, DO_ROW ? ExchangeFloats<W>::value : 0);
   extern __shared__ float smem[];
   float* tile = smem;
@@ -226,7 +242,7 @@ __global__ void __launch_bounds__(kThreads) k_full(TileArgs a) {
 // Column strips: H rows x TC columns of one array (row pitch W in global memory).
 template <int H, int W, int TC, int MODE>
 __global__ void __launch_bounds__(kThreads) k_colstrip(TileArgs a) {
-  constexpr int P = pitch_of(H, TC, true);
+  constexpr int P = strip_pitch(H, TC);
   constexpr int STRIPS = W / TC;
   extern __shared__ float smem[];
   float* tile = smem;
@@ -282,17 +298,22 @@ struct Geometry {
   static constexpr int kSmemFull = full_smem(kArrays);
   // 2-pass class
   static constexpr int strip_smem(int tc) {
+    return (round4(H * strip_pitch(H, tc)) + round4(kWarps * ExchangeFloats<H>::value) + TableFloats<H>::value) * 4;
+  }
+  // The strip width is sized with pitch tc + 4 even where the strip uses tc + 2: 256-point strips
+  // widened to 64 columns by the smaller pitch measured 4-11% slower.
+  static constexpr int sizing_smem(int tc) {
     return (round4(H * pitch_of(H, tc, true)) + round4(kWarps * ExchangeFloats<H>::value) + TableFloats<H>::value) * 4;
   }
   static constexpr int pick_tc() {
     int tc = (16384 / H) < W ? (16384 / H) : W;
-    while (tc > cmax(4, lines_per_warp<H>()) && strip_smem(tc) > kSmemTwoPerSM) tc /= 2;
+    while (tc > cmax(4, lines_per_warp<H>()) && sizing_smem(tc) > kSmemTwoPerSM) tc /= 2;
     return tc;
   }
   static constexpr int kTC = pick_tc();
   static constexpr int kSmemStrip = strip_smem(kTC);
   static constexpr int rows_smem(int rb) {
-    return (round4(rb * (W + 4)) + round4(kWarps * ExchangeFloats<W>::value) + TableFloats<W>::value) * 4;
+    return (round4(rb * rowblock_pitch(W)) + round4(kWarps * ExchangeFloats<W>::value) + TableFloats<W>::value) * 4;
   }
   static constexpr int pick_rb() {
     int rb = cmax(1, 16384 / W);

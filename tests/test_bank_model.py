@@ -1,0 +1,79 @@
+"""Shared-memory bank model of the four-step line walk (sj_lines.cuh, fs_forward).
+
+The two-pass kernels (sj_kernels.cuh) choose their tile pitches with this model: a column strip of
+256-point lines uses pitch tc + 2 and row blocks of 256- and 512-point lines use pitch w + 8 and
+w + 16.  The test recounts the wavefronts of one warp's forward four-step (Makhoul gather,
+exchange stores and loads, post-rotation stores) for those pitches and for pitch + 4, and checks
+that the chosen pitches need fewer.  A wavefront count of one warp access is the largest number of
+distinct 32-bit words that fall into one of the 32 banks.
+"""
+
+
+def wavefronts(addrs):
+    banks = {}
+    for a in addrs:
+        if a is not None:
+            banks.setdefault(a % 32, set()).add(a)
+    return max((len(s) for s in banks.values()), default=0)
+
+
+def makhoul_src(n, big_n):
+    return 2 * n if n < big_n // 2 else 2 * big_n - 1 - 2 * n
+
+
+def bitrev(b, g):
+    bits = g.bit_length() - 1
+    return int(format(b, f"0{bits}b")[::-1], 2) if bits else 0
+
+
+def four_step_wavefronts(g, pitch, rows):
+    """Wavefronts of one warp's fs_forward for G = g (line length 32 g); rows: lines are tile rows
+    (element stride 1, line stride pitch), else tile columns (element stride pitch, line stride 1)."""
+    n = 32 * g
+    lpw = 32 // g
+    xp = g + 1                                       # FourStepSizes<G>::PITCH
+    line_len = {8: 168, 16: 304}.get(g, 17 * xp)     # FourStepSizes<G>::LINE
+    plane = lpw * line_len
+    es = 1 if rows else pitch
+    base = (lambda j: j * pitch) if rows else (lambda j: j)
+    total = 0
+    for a in range(32):                               # stage-1 Makhoul gather
+        total += wavefronts([base(l // g) + makhoul_src(g * a + l % g, n) * es for l in range(32)])
+    for c in range(1, 16):                            # twiddled stage-1 outputs into the exchange
+        for pl in (0, 1):
+            total += wavefronts([pl * plane + (l // g) * line_len + l % g + c * xp for l in range(32)])
+    for col in (0, 16):                               # post rotation of columns 0 and 16
+        for side in (0, 1):
+            addrs = []
+            for l in range(32):
+                d = bitrev(l % g, g)
+                k = 32 * d + col
+                ok = d <= g // 2 if col == 0 else d < g // 2
+                if not ok or (side == 1 and (k == 0 or 2 * k == n)):
+                    addrs.append(None)
+                else:
+                    addrs.append(base(l // g) + (k if side == 0 else n - k) * es)
+            total += wavefronts(addrs)
+    ntask = lpw * 15                                  # stage 2: tasks (line, column c = 1..15)
+    for r in range(0, ntask, 32):
+        tasks = [(t // 15, 1 + t % 15) if t < ntask else None for t in range(r, r + 32)]
+        for q in range(g):
+            for pl in (0, 1):
+                total += wavefronts([None if t is None else pl * plane + t[0] * line_len + t[1] * xp + q
+                                     for t in tasks])
+        for dd in range(g):
+            for side in (0, 1):
+                total += wavefronts([None if t is None else
+                                     base(t[0]) + ((t[1] + 32 * dd) if side == 0 else n - t[1] - 32 * dd) * es
+                                     for t in tasks])
+    return total
+
+
+def test_strip_pitch_of_256_point_columns():
+    tc = 32
+    assert four_step_wavefronts(8, tc + 2, rows=False) < 0.85 * four_step_wavefronts(8, tc + 4, rows=False)
+
+
+def test_row_block_pitches_of_256_and_512_point_rows():
+    assert four_step_wavefronts(8, 256 + 8, rows=True) < 0.8 * four_step_wavefronts(8, 256 + 4, rows=True)
+    assert four_step_wavefronts(16, 512 + 16, rows=True) < 0.9 * four_step_wavefronts(16, 512 + 4, rows=True)
