@@ -359,7 +359,9 @@ def time_form(torch, lib, plan, form_id, xs, ys, batch, mode, steps, warmup, str
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 20000; 1000 for the ragged workload, whose per-array "
+                         "launch loop takes about 28 ms a step)")
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="blocks8")
@@ -372,6 +374,8 @@ def main():
     ap.add_argument("--batch", type=int, default=0,
                     help="use the first N arrays of the workload (repeated cyclically when N is larger)")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 1000 if args.workload == "ragged" else 20000
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus))
