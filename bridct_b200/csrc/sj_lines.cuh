@@ -107,6 +107,37 @@ struct FourStepSizes {
   static constexpr int FLOATS = 2 * PLANE;
 };
 
+// Exchange slot of the warp's line j, and the stage-2 task (line g2, column c) of a lane in
+// round r.  For G = 8 (4 lines per warp, 60 tasks) each of the two rounds takes the 15 columns of
+// two lines whose slots lie 16 banks apart (slot stride 168 = 8 mod 32), so a round's exchange
+// accesses are conflict-free: rows pair lines {0, 2} and {1, 3} (at a row pitch = 8 mod 32 their
+// post-rotation stores are 16 banks apart too), columns pair the adjacent columns {0, 1} and
+// {2, 3}, which the slot permutation puts on slots {0, 2} and {1, 3}.  Other G: slot = line and
+// task = lane + 32 r.
+template <int G>
+__device__ __forceinline__ int fs_slot(int j, bool rows) {
+  return (G == 8 && !rows) ? (((j & 1) << 1) | (j >> 1)) : j;
+}
+template <int G>
+struct FsTasks {
+  static constexpr int ROUNDS = G == 8 ? 2 : (FourStepSizes<G>::LPW * 15 + 31) / 32;
+  static __device__ __forceinline__ bool get(int lane, int r, bool rows, int& g2, int& c) {
+    if constexpr (G == 8) {
+      if (lane >= 30) return false;
+      const int hi = lane >= 15 ? 1 : 0;
+      c = 1 + lane - 15 * hi;
+      g2 = rows ? 2 * hi + r : 2 * r + hi;
+      return true;
+    } else {
+      const int task = lane + 32 * r;
+      if (task >= FourStepSizes<G>::LPW * 15) return false;
+      g2 = task / 15;
+      c = 1 + task % 15;
+      return true;
+    }
+  }
+};
+
 __device__ __forceinline__ int makhoul_src(int n, int N) {
   return n < N / 2 ? 2 * n : 2 * N - 1 - 2 * n;
 }
@@ -204,7 +235,7 @@ __device__ __forceinline__ void fs_forward(const LinePtr& line_ptr, int es, floa
 #pragma unroll
     for (int a = 0; a < 32; ++a) xin[a] = line[makhoul_src(G * a + b, N) * es];
     sj_rfft_32(xin, w);
-    float* re = xb + grp * SZ::LINE + b;
+    float* re = xb + fs_slot<G>(grp, es == 1) * SZ::LINE + b;
     float* im = re + SZ::PLANE;
 #pragma unroll
     for (int c = 1; c < 16; ++c) {
@@ -250,10 +281,12 @@ __device__ __forceinline__ void fs_forward(const LinePtr& line_ptr, int es, floa
       }
     }
   } else {
-    for (int task = lane; task < SZ::LPW * 15; task += 32) {
-      const int g2 = task / 15, c = 1 + task % 15;
+#pragma unroll 1
+    for (int r = 0; r < FsTasks<G>::ROUNDS; ++r) {
+      int g2, c;
+      if (!FsTasks<G>::get(lane, r, es == 1, g2, c)) continue;
       float* line = line_ptr(g2);
-      const float* re = xb + g2 * SZ::LINE + c * SZ::PITCH;
+      const float* re = xb + fs_slot<G>(g2, es == 1) * SZ::LINE + c * SZ::PITCH;
       const float* im = re + SZ::PLANE;
       float z[2 * G];
 #pragma unroll
@@ -318,10 +351,12 @@ __device__ __forceinline__ void fs_inverse(const LinePtr& line_ptr, int es, floa
       }
     }
   } else {
-    for (int task = lane; task < SZ::LPW * 15; task += 32) {
-      const int g2 = task / 15, c = 1 + task % 15;
+#pragma unroll 1
+    for (int r = 0; r < FsTasks<G>::ROUNDS; ++r) {
+      int g2, c;
+      if (!FsTasks<G>::get(lane, r, es == 1, g2, c)) continue;
       const float* line = line_ptr(g2);
-      float* re = xb + g2 * SZ::LINE + c * SZ::PITCH;
+      float* re = xb + fs_slot<G>(g2, es == 1) * SZ::LINE + c * SZ::PITCH;
       float* im = re + SZ::PLANE;
       float z[2 * G];
 #pragma unroll
@@ -336,7 +371,7 @@ __device__ __forceinline__ void fs_inverse(const LinePtr& line_ptr, int es, floa
   }
   __syncwarp();
   {
-    const float* re = xb + grp * SZ::LINE + b;
+    const float* re = xb + fs_slot<G>(grp, es == 1) * SZ::LINE + b;
     const float* im = re + SZ::PLANE;
     float w[32], xo[32];
     w[0] = w0;

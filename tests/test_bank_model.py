@@ -2,9 +2,10 @@
 
 The two-pass kernels (sj_kernels.cuh) choose their tile pitches with this model: a column strip of
 256-point lines uses pitch tc + 2 and row blocks of 256- and 512-point lines use pitch w + 8 and
-w + 16.  The test recounts the wavefronts of one warp's forward four-step (Makhoul gather,
-exchange stores and loads, post-rotation stores) for those pitches and for pitch + 4, and checks
-that the chosen pitches need fewer.  A wavefront count of one warp access is the largest number of
+w + 16.  For 256-point lines (G = 8) the stage-2 rounds pair lines whose exchange slots lie 16
+banks apart (fs_slot / FsTasks in sj_lines.cuh).  The tests recount the wavefronts of one warp's
+forward four-step (Makhoul gather, exchange stores and loads, post-rotation stores) and check that
+the chosen pitches and the paired rounds need fewer than pitch + 4 and rounds of consecutive tasks.  A wavefront count of one warp access is the largest number of
 distinct 32-bit words that fall into one of the 32 banks.
 """
 
@@ -26,9 +27,24 @@ def bitrev(b, g):
     return int(format(b, f"0{bits}b")[::-1], 2) if bits else 0
 
 
-def four_step_wavefronts(g, pitch, rows):
+def fs_slot(g, j, rows):
+    return (((j & 1) << 1) | (j >> 1)) if (g == 8 and not rows) else j
+
+
+def rounds_of(g, rows, paired):
+    """Stage-2 (line, column) task of each lane, per round."""
+    lpw = 32 // g
+    if g == 8 and paired:
+        return [[((2 * (l // 15) + r) if rows else (2 * r + l // 15), 1 + l % 15) if l < 30 else None
+                 for l in range(32)] for r in range(2)]
+    ntask = lpw * 15
+    return [[(t // 15, 1 + t % 15) if t < ntask else None for t in range(r, r + 32)] for r in range(0, ntask, 32)]
+
+
+def four_step_wavefronts(g, pitch, rows, paired=True):
     """Wavefronts of one warp's fs_forward for G = g (line length 32 g); rows: lines are tile rows
-    (element stride 1, line stride pitch), else tile columns (element stride pitch, line stride 1)."""
+    (element stride 1, line stride pitch), else tile columns (element stride pitch, line stride 1).
+    paired: the kernel's stage-2 rounds and exchange slots; else consecutive tasks, slot = line."""
     n = 32 * g
     lpw = 32 // g
     xp = g + 1                                       # FourStepSizes<G>::PITCH
@@ -36,12 +52,13 @@ def four_step_wavefronts(g, pitch, rows):
     plane = lpw * line_len
     es = 1 if rows else pitch
     base = (lambda j: j * pitch) if rows else (lambda j: j)
+    slot = (lambda j: fs_slot(g, j, rows)) if paired else (lambda j: j)
     total = 0
     for a in range(32):                               # stage-1 Makhoul gather
         total += wavefronts([base(l // g) + makhoul_src(g * a + l % g, n) * es for l in range(32)])
     for c in range(1, 16):                            # twiddled stage-1 outputs into the exchange
         for pl in (0, 1):
-            total += wavefronts([pl * plane + (l // g) * line_len + l % g + c * xp for l in range(32)])
+            total += wavefronts([pl * plane + slot(l // g) * line_len + l % g + c * xp for l in range(32)])
     for col in (0, 16):                               # post rotation of columns 0 and 16
         for side in (0, 1):
             addrs = []
@@ -54,12 +71,10 @@ def four_step_wavefronts(g, pitch, rows):
                 else:
                     addrs.append(base(l // g) + (k if side == 0 else n - k) * es)
             total += wavefronts(addrs)
-    ntask = lpw * 15                                  # stage 2: tasks (line, column c = 1..15)
-    for r in range(0, ntask, 32):
-        tasks = [(t // 15, 1 + t % 15) if t < ntask else None for t in range(r, r + 32)]
+    for tasks in rounds_of(g, rows, paired):          # stage 2: tasks (line, column c = 1..15)
         for q in range(g):
             for pl in (0, 1):
-                total += wavefronts([None if t is None else pl * plane + t[0] * line_len + t[1] * xp + q
+                total += wavefronts([None if t is None else pl * plane + slot(t[0]) * line_len + t[1] * xp + q
                                      for t in tasks])
         for dd in range(g):
             for side in (0, 1):
@@ -77,3 +92,8 @@ def test_strip_pitch_of_256_point_columns():
 def test_row_block_pitches_of_256_and_512_point_rows():
     assert four_step_wavefronts(8, 256 + 8, rows=True) < 0.8 * four_step_wavefronts(8, 256 + 4, rows=True)
     assert four_step_wavefronts(16, 512 + 16, rows=True) < 0.9 * four_step_wavefronts(16, 512 + 4, rows=True)
+
+
+def test_paired_stage2_rounds_of_256_point_lines():
+    for rows, pitch in ((True, 256 + 8), (False, 32 + 2), (False, 32 + 4)):
+        assert four_step_wavefronts(8, pitch, rows) < 0.9 * four_step_wavefronts(8, pitch, rows, paired=False)
