@@ -45,8 +45,8 @@ struct RaggedArgs {
 };
 
 constexpr int kRaggedThreads = 256;                                 // 2 CTAs per SM at <= 128 registers
-// Exchange floats per warp, worst case over the four-step widths G = 4..32 (G = 4 needs most:
-// 8 lines x 17 columns x pitch 5 x re/im).
+// Exchange floats per warp, worst case over the four-step widths G = 4..32 (G = 4 and 8 need
+// most: 8 slots of 84 or 4 slots of 168 floats, re and im).
 constexpr int kXbufPerWarp = cmax(cmax(FourStepSizes<4>::FLOATS, FourStepSizes<8>::FLOATS),
                                   cmax(FourStepSizes<16>::FLOATS, FourStepSizes<32>::FLOATS));
 constexpr int kRaggedXbuf = (kRaggedThreads / 32) * kXbufPerWarp;

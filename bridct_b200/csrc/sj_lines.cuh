@@ -100,33 +100,35 @@ template <int G>
 struct FourStepSizes {
   static constexpr int LPW = 32 / G;           // lines per warp
   static constexpr int PITCH = G + 1;          // odd pitch: conflict-free column reads
-  // per-line stride: padded for G = 8, 16 so that the LPW lines' stage-1 writes hit disjoint
-  // banks (stride == G * odd mod 32); G = 4 stays unpadded to keep the 8-line buffer small
-  static constexpr int LINE = G == 8 ? 168 : G == 16 ? 304 : 17 * PITCH;
+  // per-line (slot) stride: the LPW slots' stage-1 writes hit disjoint banks (stride = G * odd
+  // mod 32), and for G = 4, 8 slots LPW/2 apart lie 16 banks apart (stride * LPW/2 = 16 mod 32)
+  static constexpr int LINE = G == 4 ? 84 : G == 8 ? 168 : G == 16 ? 304 : 17 * PITCH;
   static constexpr int PLANE = LPW * LINE;
   static constexpr int FLOATS = 2 * PLANE;
 };
 
 // Exchange slot of the warp's line j, and the stage-2 task (line g2, column c) of a lane in
-// round r.  For G = 8 (4 lines per warp, 60 tasks) each of the two rounds takes the 15 columns of
-// two lines whose slots lie 16 banks apart (slot stride 168 = 8 mod 32), so a round's exchange
-// accesses are conflict-free: rows pair lines {0, 2} and {1, 3} (at a row pitch = 8 mod 32 their
-// post-rotation stores are 16 banks apart too), columns pair the adjacent columns {0, 1} and
-// {2, 3}, which the slot permutation puts on slots {0, 2} and {1, 3}.  Other G: slot = line and
-// task = lane + 32 r.
+// round r.  For G = 4 and 8 (LPW = 8 or 4 lines per warp) each of the LPW/2 rounds takes the 15
+// columns of two lines whose slots lie LPW/2 apart, i.e. 16 banks apart, so a round's exchange
+// accesses are conflict-free.  Rows pair lines r and r + LPW/2 (at a row pitch of 4 mod 8 for
+// G = 4, 8 mod 32 for G = 8 their post-rotation stores are 16 banks apart too); columns pair the
+// adjacent columns 2r and 2r + 1, which the slot permutation puts LPW/2 slots apart.  Other G:
+// slot = line and task = lane + 32 r.
 template <int G>
 __device__ __forceinline__ int fs_slot(int j, bool rows) {
-  return (G == 8 && !rows) ? (((j & 1) << 1) | (j >> 1)) : j;
+  constexpr int HALF = FourStepSizes<G>::LPW / 2;
+  return ((G == 4 || G == 8) && !rows) ? (j >> 1) + HALF * (j & 1) : j;
 }
 template <int G>
 struct FsTasks {
-  static constexpr int ROUNDS = G == 8 ? 2 : (FourStepSizes<G>::LPW * 15 + 31) / 32;
+  static constexpr bool PAIRED = G == 4 || G == 8;
+  static constexpr int ROUNDS = PAIRED ? FourStepSizes<G>::LPW / 2 : (FourStepSizes<G>::LPW * 15 + 31) / 32;
   static __device__ __forceinline__ bool get(int lane, int r, bool rows, int& g2, int& c) {
-    if constexpr (G == 8) {
+    if constexpr (PAIRED) {
       if (lane >= 30) return false;
       const int hi = lane >= 15 ? 1 : 0;
       c = 1 + lane - 15 * hi;
-      g2 = rows ? 2 * hi + r : 2 * r + hi;
+      g2 = rows ? r + (FourStepSizes<G>::LPW / 2) * hi : 2 * r + hi;
       return true;
     } else {
       const int task = lane + 32 * r;

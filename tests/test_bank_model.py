@@ -2,8 +2,8 @@
 
 The two-pass kernels (sj_kernels.cuh) choose their tile pitches with this model: a column strip of
 256-point lines uses pitch tc + 2 and row blocks of 256- and 512-point lines use pitch w + 8 and
-w + 16.  For 256-point lines (G = 8) the stage-2 rounds pair lines whose exchange slots lie 16
-banks apart (fs_slot / FsTasks in sj_lines.cuh).  The tests recount the wavefronts of one warp's
+w + 16.  For 128- and 256-point lines (G = 4, 8) the stage-2 rounds pair lines whose exchange slots lie
+16 banks apart (fs_slot / FsTasks in sj_lines.cuh).  The tests recount the wavefronts of one warp's
 forward four-step (Makhoul gather, exchange stores and loads, post-rotation stores) and check that
 the chosen pitches and the paired rounds need fewer than pitch + 4 and rounds of consecutive tasks.  A wavefront count of one warp access is the largest number of
 distinct 32-bit words that fall into one of the 32 banks.
@@ -28,15 +28,16 @@ def bitrev(b, g):
 
 
 def fs_slot(g, j, rows):
-    return (((j & 1) << 1) | (j >> 1)) if (g == 8 and not rows) else j
+    half = 32 // g // 2
+    return (j >> 1) + half * (j & 1) if (g in (4, 8) and not rows) else j
 
 
 def rounds_of(g, rows, paired):
     """Stage-2 (line, column) task of each lane, per round."""
     lpw = 32 // g
-    if g == 8 and paired:
-        return [[((2 * (l // 15) + r) if rows else (2 * r + l // 15), 1 + l % 15) if l < 30 else None
-                 for l in range(32)] for r in range(2)]
+    if g in (4, 8) and paired:
+        return [[((r + lpw // 2 * (l // 15)) if rows else (2 * r + l // 15), 1 + l % 15) if l < 30 else None
+                 for l in range(32)] for r in range(lpw // 2)]
     ntask = lpw * 15
     return [[(t // 15, 1 + t % 15) if t < ntask else None for t in range(r, r + 32)] for r in range(0, ntask, 32)]
 
@@ -48,7 +49,7 @@ def four_step_wavefronts(g, pitch, rows, paired=True):
     n = 32 * g
     lpw = 32 // g
     xp = g + 1                                       # FourStepSizes<G>::PITCH
-    line_len = {8: 168, 16: 304}.get(g, 17 * xp)     # FourStepSizes<G>::LINE
+    line_len = {4: 84, 8: 168, 16: 304}.get(g, 17 * xp)   # FourStepSizes<G>::LINE
     plane = lpw * line_len
     es = 1 if rows else pitch
     base = (lambda j: j * pitch) if rows else (lambda j: j)
@@ -94,6 +95,8 @@ def test_row_block_pitches_of_256_and_512_point_rows():
     assert four_step_wavefronts(16, 512 + 16, rows=True) < 0.9 * four_step_wavefronts(16, 512 + 4, rows=True)
 
 
-def test_paired_stage2_rounds_of_256_point_lines():
+def test_paired_stage2_rounds_of_128_and_256_point_lines():
     for rows, pitch in ((True, 256 + 8), (False, 32 + 2), (False, 32 + 4)):
         assert four_step_wavefronts(8, pitch, rows) < 0.9 * four_step_wavefronts(8, pitch, rows, paired=False)
+    for rows, pitch in ((True, 128 + 4), (False, 64 + 4)):
+        assert four_step_wavefronts(4, pitch, rows) < 0.8 * four_step_wavefronts(4, pitch, rows, paired=False)
