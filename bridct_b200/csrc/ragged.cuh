@@ -95,11 +95,42 @@ __device__ __forceinline__ int ragged_pitch(int rows, int cols, bool column_pass
   return cols + 4;
 }
 
-// Loads rows x cols floats (row pitch gp in global) into shared memory (pitch P).
+__device__ __forceinline__ void rg_cp_async16(float* dst, const float* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+               "l"(src) : "memory");
+}
+__device__ __forceinline__ void rg_cp_async4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+               "l"(src) : "memory");
+}
+
+// Loads rows x cols floats (row pitch gp in global) into shared memory (pitch P).  The copies are
+// asynchronous (cp.async), so a thread has all of its share of the block in flight at once; the
+// caller's __syncthreads after this call publishes the block.  An odd-pitch block copies 4-byte
+// elements (its rows are not 16-byte aligned), except when it must bypass L1 (row blocks read data
+// that other CTAs wrote in this launch; 4-byte cp.async always goes through L1), where it loads
+// through L2 synchronously.
 __device__ __forceinline__ void load_block(const float* g, long long gp, int rows, int cols, float* s, int P,
                                            bool bypass_l1) {
   const int q = cols >> 2;
   const bool vec = (P & 3) == 0;
+  if (vec || !bypass_l1) {
+    for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
+      const int r = i / q, c = (i % q) * 4;
+      const float* src = g + r * gp + c;
+      float* d = s + r * P + c;
+      if (vec) {
+        rg_cp_async16(d, src);
+      } else {
+        rg_cp_async4(d, src);
+        rg_cp_async4(d + 1, src + 1);
+        rg_cp_async4(d + 2, src + 2);
+        rg_cp_async4(d + 3, src + 3);
+      }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    return;
+  }
   for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
     const int r = i / q, c = (i % q) * 4;
     const float4* p = reinterpret_cast<const float4*>(g + r * gp + c);
