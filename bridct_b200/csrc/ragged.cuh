@@ -95,15 +95,6 @@ __device__ __forceinline__ int ragged_pitch(int rows, int cols, bool column_pass
   return cols + 4;
 }
 
-__device__ __forceinline__ void rg_cp_async16(float* dst, const float* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
-               "l"(src) : "memory");
-}
-__device__ __forceinline__ void rg_cp_async4(float* dst, const float* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
-               "l"(src) : "memory");
-}
-
 // Loads rows x cols floats (row pitch gp in global) into shared memory (pitch P).  The copies are
 // asynchronous (cp.async), so a thread has all of its share of the block in flight at once; the
 // caller's __syncthreads after this call publishes the block.  An odd-pitch block copies 4-byte
@@ -120,15 +111,15 @@ __device__ __forceinline__ void load_block(const float* g, long long gp, int row
       const float* src = g + r * gp + c;
       float* d = s + r * P + c;
       if (vec) {
-        rg_cp_async16(d, src);
+        cp_async16(d, src);
       } else {
-        rg_cp_async4(d, src);
-        rg_cp_async4(d + 1, src + 1);
-        rg_cp_async4(d + 2, src + 2);
-        rg_cp_async4(d + 3, src + 3);
+        cp_async4(d, src);
+        cp_async4(d + 1, src + 1);
+        cp_async4(d + 2, src + 2);
+        cp_async4(d + 3, src + 3);
       }
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    cp_async_wait_all();
     return;
   }
   for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
