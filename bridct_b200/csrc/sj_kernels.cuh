@@ -87,7 +87,11 @@ __host__ __device__ constexpr int pitch_of(int h, int w, bool has_col) { return 
 // a column strip of 256-point lines with pitch tc + 2 (= 2 mod 4) and row blocks of 256- and
 // 512-point lines with pitch w + 8 (= 8 mod 32) and w + 16 (= 16 mod 32) need 20%, 23% and 14%
 // fewer wavefronts per line than with pitch + 4; tc + 2 rows are staged with 64-bit accesses.
-__host__ __device__ constexpr int strip_pitch(int h, int tc) { return h == 256 ? tc + 2 : pitch_of(h, tc, true); }
+// 32-column strips of 512-point lines take pitch 34: as few wavefronts as the odd pitch 33, and an
+// even pitch lets tile_load copy asynchronously.
+__host__ __device__ constexpr int strip_pitch(int h, int tc) {
+  return h == 256 || (h == 512 && tc == 32) ? tc + 2 : pitch_of(h, tc, true);
+}
 __host__ __device__ constexpr int rowblock_pitch(int w) { return w == 256 ? w + 8 : w == 512 ? w + 16 : w + 4; }
 
 // Asynchronous global -> shared copies (cp.async; 16 bytes through L2 only, 8 and 4 bytes through

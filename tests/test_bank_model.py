@@ -100,3 +100,8 @@ def test_paired_stage2_rounds_of_128_and_256_point_lines():
         assert four_step_wavefronts(8, pitch, rows) < 0.9 * four_step_wavefronts(8, pitch, rows, paired=False)
     for rows, pitch in ((True, 128 + 4), (False, 64 + 4)):
         assert four_step_wavefronts(4, pitch, rows) < 0.8 * four_step_wavefronts(4, pitch, rows, paired=False)
+
+
+def test_even_pitch_of_512_point_strips_costs_no_more_than_the_odd_one():
+    # 32-column strips of 512-point lines use pitch 34 instead of 33 so that they load asynchronously
+    assert four_step_wavefronts(16, 34, rows=False) <= four_step_wavefronts(16, 33, rows=False)
