@@ -240,11 +240,13 @@ __global__ void __launch_bounds__(kThreads) k_full(TileArgs a) {
     const long long left = a.rows_total - t * (long long)TR;
     return left >= TR ? TR : (int)left;
   };
-  // Whole-array tiles with a four-step axis, and row passes of 128..512-point lines, are
-  // latency-bound: they prefetch the next tile into registers during the transform (measured
-  // +10-50% on such shapes).  Register-line kernels and 1024-point rows keep their occupancy
-  // instead (prefetching cost them up to 18%).
-  constexpr bool kPrefetch = DO_COL ? DO_ROW && (H >= 128 || W >= 128) : (DO_ROW && W >= 128 && W <= 512);
+  // Whole-array tiles with a 128..1024-point axis and row passes of 128-point lines prefetch the
+  // next tile into registers during the transform (measured +10-50% on such shapes).  Full
+  // 16384-float tiles whose rows are the long axis (64x256, 32x512, 16x1024, 64 prefetch floats a
+  // thread) and row passes of 256..1024-point lines load with cp.async instead: measured +3-27%
+  // and +1-11% over the register prefetch there.  Short-line tiles keep their occupancy.
+  constexpr bool kPrefetch = DO_COL ? DO_ROW && (H >= 128 || W >= 128) && !(W >= 256 && TR * W >= 16384)
+                                    : (DO_ROW && W == 128);
   TileRegs<P, kPrefetch ? TR : 4, kPrefetch ? W : 4> next;
   if (kPrefetch && blockIdx.x < a.ntiles) next.load(a.x + blockIdx.x * (long long)TR * W, W, rows_of(blockIdx.x));
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
