@@ -157,6 +157,8 @@ __device__ __forceinline__ void bulk_wait_read0() {
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// Waits until at most one committed bulk group is still reading shared memory.
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -336,7 +338,10 @@ __device__ __forceinline__ void issue_mmas(uint32_t sstage, uint32_t sabuf, uint
 //   warps 4-7      split group 0: even tiles, ring tile s -> A buffer 0  (waits stage_full, a_free)
 //   warps 8-11     split group 1: odd tiles, ring tile s -> A buffer 1
 //   warps 12-15    epilogue: acc t -> ring tile s (16 columns at a time) -> TMA store
-//                  (waits acc_full; frees acc t, then ring tile s once the store has read it)
+//                  (waits acc_full; frees acc t, then ring tile s once the store has read it;
+//                  BF16x3, with its 5-tile ring, frees ring tile s one tile later so that the
+//                  store's read overlaps the next tile's epilogue: +9% on the block batch, while
+//                  TF32x3's 4-tile ring measured 8% slower with the later release)
 // Tile j of this CTA uses ring tile j % kStages, A buffer j % 2 and accumulator j % 2.  The split
 // is the longest role per tile, so two groups (one warp per sub-partition each) alternate.
 constexpr int kTc8Threads = 512;
@@ -499,11 +504,24 @@ __global__ void __launch_bounds__(kTc8Threads, 1) k_tc8(const __grid_constant__ 
         tma_store_2d(&ymap, 0, tile * kRows, sbase + L::kStageOff + s * kTile);
         tma_store_2d(&ymap, 32, tile * kRows, sbase + L::kStageOff + s * kTile + 16384u);
         bulk_commit();
-        bulk_wait_read0();
-        mbar_arrive(bars.stage_free + 8 * s);
+        if constexpr (FORM == BF16X3) {
+          if (j > 0) {               // the previous tile's store has read its ring tile
+            bulk_wait_read1();
+            mbar_arrive(bars.stage_free + 8 * ((j - 1) % kStages));
+          }
+        } else {
+          bulk_wait_read0();
+          mbar_arrive(bars.stage_free + 8 * s);
+        }
       }
     }
-    if (r == 0) bulk_wait0();
+    if (r == 0) {
+      if (FORM == BF16X3 && ok && ntile_local > 0) {
+        bulk_wait_read0();
+        mbar_arrive(bars.stage_free + 8 * ((ntile_local - 1) % kStages));
+      }
+      bulk_wait0();
+    }
   }
   if (!ok) {
     s_abort = 1;
