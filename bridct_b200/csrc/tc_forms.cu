@@ -443,7 +443,9 @@ int fp8_refined(const bridct_plan* p, bool inverse, const float* src, float* dst
 
 int apply_fp8(bridct_plan* p, int mode, const float* x, float* y, size_t batch, cudaStream_t st, TcDevice* d) {
   const size_t elems = p->elements;
-  size_t chunk = (size_t(16) << 20) / (elems * sizeof(float));
+  // Chunks of 64 MB: the twelve launches of a refined transform dominate smaller chunks (16 MB
+  // measured 304 GB/s on 2048 arrays of 256x256, 32 MB 344, 64 MB 352, with the same outputs).
+  size_t chunk = (size_t(64) << 20) / (elems * sizeof(float));
   if (chunk < 1) chunk = 1;
   if (chunk > batch) chunk = batch;
   const size_t ce = chunk * elems;
