@@ -198,3 +198,13 @@ def test_fp8_no_write_past_batch_and_rejects_other_shapes():
     z = torch.randn(2, 64, 64, device="cuda")
     assert L.bridct_plan_apply_form_device(plan64, 0, _lib.FORM_TC_FP8, z.data_ptr(), z.data_ptr() + 0, 1,
                                            None) in (_lib.INVALID_ARGUMENT, _lib.OVERLAPPING_BUFFERS)
+
+
+def test_fp8_batch_across_chunks_matches_small_batches_bitwise():
+    # 600 arrays of 128x256 span two of the FP8 form's 64 MB chunks; quantization scales are per
+    # 32x32 tile and the passes are per row, so every array's result is independent of the cut
+    x = torch.randn(600, 128, 256, device="cuda")
+    y = torch_api.apply(x, 0, form="tc_fp8")
+    part = torch_api.apply(x[508:516].clone(), 0, form="tc_fp8")
+    torch.cuda.synchronize()
+    assert torch.equal(y[508:516], part)
