@@ -22,7 +22,7 @@ CANDIDATES: Dict[str, Sequence[int]] = {
     "tile_floats": (1024, 2048, 4096, 8192, 16384),
     "strip_floats": (2048, 4096, 8192, 16384),
     "row_floats": (2048, 4096, 8192, 16384),
-    "lookahead": (1, 2, 4, 8, 16),
+    "lookahead": (1, 2, 4, 8, 16, 32, 64),
 }
 
 
