@@ -123,7 +123,6 @@ DeviceCtx* device_ctx(int device) {
   d->l2_bytes = prop.l2CacheSize;
   d->launch.sm_count = prop.multiProcessorCount;
   // Two-pass chunk: a quarter of L2 keeps the column pass's output resident for the row pass.
-  d->launch.l2_chunk_bytes = std::max<long long>(4ll << 20, prop.l2CacheSize / 4);
   PlainLauncher (*tab)[8][3] = d->plain;
   plain_table_h8(tab[0]);
   plain_table_h16(tab[1]);

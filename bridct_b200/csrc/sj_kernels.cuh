@@ -7,10 +7,9 @@
 //                           One HBM read and one HBM write per element.
 //   h*w >  16384  "2-pass"  k_colstrip (h rows x TC columns per CTA, column lines, x -> y)
 //                           then k_full<DO_COL=0> (TR full rows per CTA, row lines, y -> y in
-//                           place).  The intermediate lives in y and is re-read while it is
-//                           still L2-resident: the host walks large batches in chunks sized
-//                           for L2 (the reference's rect route does the same pair of passes,
-//                           vertical then bands, src/generated/rect.c:5-23).
+//                           place), one launch each over the whole batch.  The intermediate
+//                           lives in y (the reference's rect route does the same pair of
+//                           passes, vertical then bands, src/generated/rect.c:5-23).
 // Shared-memory rows use an odd pitch (w + 1 floats) so that a thread-per-row line walk and a
 // thread-per-column line walk are both bank-conflict free.
 #pragma once

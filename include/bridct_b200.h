@@ -28,7 +28,7 @@ enum bridct_form {
 BRIDCT_API const char *bridct_last_error(void);
 
 /* GPU schedule of the plan: "sj-tile" (both passes in shared memory) or
- * "sj-two-pass" (column pass then row pass through L2).  NULL for a NULL plan. */
+ * "sj-two-pass" (column pass then row pass).  NULL for a NULL plan. */
 BRIDCT_API const char *bridct_plan_gpu_route(const bridct_plan *plan);
 
 /* `batch` contiguous h*w arrays; host (pageable or pinned) or device pointers.
