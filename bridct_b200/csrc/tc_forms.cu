@@ -443,9 +443,10 @@ int fp8_refined(const bridct_plan* p, bool inverse, const float* src, float* dst
 
 int apply_fp8(bridct_plan* p, int mode, const float* x, float* y, size_t batch, cudaStream_t st, TcDevice* d) {
   const size_t elems = p->elements;
-  // Chunks of 64 MB: the twelve launches of a refined transform dominate smaller chunks (16 MB
-  // measured 304 GB/s on 2048 arrays of 256x256, 32 MB 344, 64 MB 352, with the same outputs).
-  size_t chunk = (size_t(64) << 20) / (elems * sizeof(float));
+  // Chunks of 256 MB: the twelve launches of a refined transform dominate smaller chunks (2048
+  // arrays of 256x256, same outputs: 16 MB 304 GB/s, 32 MB 344, 64 MB 352-366, 256 MB 382,
+  // 1 GB 389); the scratch needs about 17 bytes per element of a chunk.
+  size_t chunk = (size_t(256) << 20) / (elems * sizeof(float));
   if (chunk < 1) chunk = 1;
   if (chunk > batch) chunk = batch;
   const size_t ce = chunk * elems;
@@ -493,7 +494,11 @@ int log2i(int v) {
   return r;
 }
 
-constexpr size_t kSepChunkBytes = size_t(48) << 20;   // arrays per pass pair: about 48 MB
+// Arrays per pass pair: up to 1 GB, so that batches up to that size run each pass as one launch.
+// Chunks of 48 MB kept the intermediate in L2 but measured slower (2048 x 256^2: BF16x3 826 ->
+// 962, TF32x3 565 -> 680 GB/s): the passes are bound by the shared-memory port, not by HBM, and
+// every chunk adds launch tails.  The plan-owned scratch holds one chunk.
+constexpr size_t kSepChunkBytes = size_t(1024) << 20;
 
 // Separable form: per batch of arrays, pass 1 (rows of W) x -> scratch, pass 2 (rows of H)
 // scratch -> y; the round trip runs the forward pair then the inverse pair on the same batch.

@@ -49,7 +49,9 @@ BRIDCT_API int bridct_plan_apply_device(bridct_plan *plan, enum bridct_mode mode
  * on the tensor cores; see enum bridct_form for the shapes each form supports).  The
  * tensor-core forms on axes of 64..256 and the FP8 form keep their intermediate in scratch
  * owned by the plan (allocated by the first call that needs it, so make that call before any
- * stream capture): calls on one plan must not run concurrently on different streams. */
+ * stream capture): calls on one plan must not run concurrently on different streams.  The
+ * scratch holds one chunk of the batch and grows with the largest batch a plan has seen: up
+ * to 1 GB for BF16x3/TF32x3, about 17 bytes per element of up to 256 MB of input for FP8. */
 BRIDCT_API int bridct_plan_apply_form_device(bridct_plan *plan, enum bridct_mode mode,
                                              enum bridct_form form, const float *input,
                                              float *output, size_t batch, void *stream);

@@ -104,13 +104,18 @@ def test_tcsep_matches_fp64(form, shape):
 
 
 @pytest.mark.parametrize("form", FORMS)
-def test_tcsep_spans_several_l2_batches(form):
-    # 256x256 arrays are cut into batches of 192 per pass pair; 401 arrays take three
-    x = np.random.default_rng(7).standard_normal((401, 256, 256)).astype(np.float32)
-    y = run(x, 0, form)
-    idx = [0, 191, 192, 383, 384, 400]
-    ref = O.fp64_apply(x[idx], 0)
-    assert O.rel_max_error(y[idx], ref, x[idx], output_scaled=True) <= TOL
+def test_tcsep_spans_several_chunks(form):
+    # 256x256 arrays are cut into chunks of 4096 (1 GB) per pass pair; 8200 arrays take three
+    g = torch.Generator(device="cuda").manual_seed(7)
+    x = torch.randn(8200, 256, 256, device="cuda", generator=g)
+    y = torch_api.apply(x, 0, form=form)
+    torch.cuda.synchronize()
+    assert _lib.lib().bridct_device_timeout_flag(torch.cuda.current_device()) == 0
+    idx = [0, 4095, 4096, 8191, 8192, 8199]
+    xs, ys = x[idx].cpu().numpy(), y[idx].cpu().numpy()
+    del x, y
+    ref = O.fp64_apply(xs, 0)
+    assert O.rel_max_error(ys, ref, xs, output_scaled=True) <= TOL
 
 
 @pytest.mark.parametrize("form", FORMS)
@@ -201,10 +206,11 @@ def test_fp8_no_write_past_batch_and_rejects_other_shapes():
 
 
 def test_fp8_batch_across_chunks_matches_small_batches_bitwise():
-    # 600 arrays of 128x256 span two of the FP8 form's 64 MB chunks; quantization scales are per
-    # 32x32 tile and the passes are per row, so every array's result is independent of the cut
-    x = torch.randn(600, 128, 256, device="cuda")
+    # 2100 arrays of 128x256 span two of the FP8 form's 256 MB chunks (2048 arrays each);
+    # quantization scales are per 32x32 tile and the passes are per row, so every array's result
+    # is independent of the cut
+    x = torch.randn(2100, 128, 256, device="cuda")
     y = torch_api.apply(x, 0, form="tc_fp8")
-    part = torch_api.apply(x[508:516].clone(), 0, form="tc_fp8")
+    part = torch_api.apply(x[2044:2052].clone(), 0, form="tc_fp8")
     torch.cuda.synchronize()
-    assert torch.equal(y[508:516], part)
+    assert torch.equal(y[2044:2052], part)
