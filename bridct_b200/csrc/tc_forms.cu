@@ -8,8 +8,8 @@
 //
 // Axes of 64, 128 and 256 (any combination): two row passes of k_tcpass per batch of arrays
 // (pass 1 over rows of length W into a plan-owned scratch, pass 2 over rows of length H into
-// the output), with the batch cut so that the scratch stays in L2 between the passes; BF16x3 on
-// 64x64 arrays runs both passes in one launch (k_tc64) with the intermediate on chip.  The B
+// the output), over chunks of up to 1 GB of arrays; BF16x3 on 64x64 arrays runs both passes in
+// one launch (k_tc64) with the intermediate on chip.  The B
 // images hold C_L (or C_L^T for the inverse) split into bf16 or tf32 parts, one 64-row slice
 // per N-block, in the K-major 128-byte-swizzled layout.
 #include <cuda.h>

@@ -6,8 +6,8 @@
 // transposed:
 //     pass 1: rows of X (R = H, L = W)      -> T_b = (X_b C_W^T)^T   (W x H per array)
 //     pass 2: rows of T (R = W, L = H)      -> Y_b = (T_b C_H^T)^T = C_H X_b C_W^T
-// so the second pass is again a plain row pass.  The host runs the passes over batches of
-// arrays small enough that T stays in L2 between them.
+// so the second pass is again a plain row pass.  The host runs the passes over chunks of up to
+// 1 GB of arrays (T is plan-owned scratch).
 //
 // One pass is a GEMM with M = rows (tiles of 128), N = L, K = L.  Each CTA owns one N-block of
 // 64 output columns: its slice of C_L (64 x L, split into bf16 or tf32 parts, in the K-major
