@@ -64,10 +64,18 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
     k<<<(unsigned)grid, kB8Threads, smem, st>>>(x, y, batch);
     return cudaGetLastError();
   } else if constexpr (Gm::kTile) {
-    auto k = k_full<H, W, Gm::kTR, true, true, MODE>;
-    const int bps = kernel_blocks_per_sm(k, Gm::kSmemFull);
-    TileArgs a{x, y, (batch * H + Gm::kTR - 1) / Gm::kTR, batch * H, tab};
-    return launch_tiles(k, Gm::kSmemFull, bps, a, ctx, st);
+    // 16384-float tiles instead of 8192 where they measured faster on 128 MiB batches: 64-wide
+    // arrays up to 64 high (+6..14%, except the 64 x 64 inverse, -2%) and forward/inverse of
+    // 8..32 x 128 (+17..22%); narrower tiles, 64 x 128 and those round trips measured 5..21%
+    // slower with them.
+    constexpr bool kBig = (W == 64 && H <= 64 && !(H == 64 && MODE == LM_INV)) ||
+                          (W == 128 && H <= 32 && MODE != LM_RT);
+    constexpr int TR = kBig ? Gm::kTRBig : Gm::kTR;
+    constexpr int smem = kBig ? Gm::kSmemFullBig : Gm::kSmemFull;
+    auto k = k_full<H, W, TR, true, true, MODE>;
+    const int bps = kernel_blocks_per_sm(k, smem);
+    TileArgs a{x, y, (batch * H + TR - 1) / TR, batch * H, tab};
+    return launch_tiles(k, smem, bps, a, ctx, st);
   } else {
     auto kc = k_colstrip<H, W, Gm::kTC, MODE>;
     auto kr = k_full<H, W, Gm::kRB, false, true, MODE>;

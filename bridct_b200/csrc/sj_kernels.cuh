@@ -322,14 +322,18 @@ struct Geometry {
     return (round4(arrays * H * pitch_of(H, W, true)) + round4(kXbufFull) + TableFloats<H>::value +
             TableFloats<W>::value) * 4;
   }
-  static constexpr int pick_arrays() {
-    int a = cmax(1, kTileFloats / (H * W));
+  static constexpr int pick_arrays(int target) {
+    int a = cmax(1, target / (H * W));
     while (a > 1 && full_smem(a) > kSmemTwoPerSM) a /= 2;
     return a;
   }
-  static constexpr int kArrays = pick_arrays();
+  static constexpr int kArrays = pick_arrays(kTileFloats);
   static constexpr int kTR = kTile ? kArrays * H : 1;
   static constexpr int kSmemFull = full_smem(kArrays);
+  // Tiles of twice the target, for the shapes where they measured faster (see launch_plain).
+  static constexpr int kArraysBig = pick_arrays(2 * kTileFloats);
+  static constexpr int kTRBig = kTile ? kArraysBig * H : 1;
+  static constexpr int kSmemFullBig = full_smem(kArraysBig);
   // 2-pass class
   static constexpr int strip_smem(int tc) {
     return (round4(H * strip_pitch(H, tc)) + round4(kWarps * ExchangeFloats<H>::value) + TableFloats<H>::value) * 4;
