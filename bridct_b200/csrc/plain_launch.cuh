@@ -23,12 +23,12 @@ static int kernel_blocks_per_sm(Kernel k, int smem, int threads = kThreads) {
 
 template <typename Kernel>
 static cudaError_t launch_tiles(Kernel k, int smem, int bps, TileArgs a, const LaunchCtx& ctx,
-                                cudaStream_t st) {
+                                cudaStream_t st, int threads = kThreads) {
   if (bps <= 0) return cudaErrorInvalidConfiguration;
   if (a.ntiles <= 0) return cudaSuccess;
   long long grid = (long long)ctx.sm_count * bps;
   if (grid > a.ntiles) grid = a.ntiles;
-  k<<<(unsigned)grid, kThreads, smem, st>>>(a);
+  k<<<(unsigned)grid, threads, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -77,10 +77,15 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
     TileArgs a{x, y, (batch * H + TR - 1) / TR, batch * H, tab};
     return launch_tiles(k, smem, bps, a, ctx, st);
   } else {
-    auto kc = k_colstrip<H, W, Gm::kTC, MODE>;
-    auto kr = k_full<H, W, Gm::kRB, false, true, MODE>;
-    const int bpc = kernel_blocks_per_sm(kc, Gm::kSmemStrip);
-    const int bpr = kernel_blocks_per_sm(kr, Gm::kSmemRows);
+    // Round trips of 128-point register lines run 128-thread CTAs without register prefetch:
+    // every warp has a line and two CTAs share an SM, which measured +8..13% over one 256-thread
+    // CTA with prefetch; forward and inverse measured 5..9% slower that way and keep 256 threads.
+    constexpr int TC_T = H == 128 && MODE == LM_RT ? 128 : kThreads;
+    constexpr int TR_T = W == 128 && MODE == LM_RT ? 128 : kThreads;
+    auto kc = k_colstrip<H, W, Gm::kTC, MODE, TC_T>;
+    auto kr = k_full<H, W, Gm::kRB, false, true, MODE, TR_T>;
+    const int bpc = kernel_blocks_per_sm(kc, Gm::kSmemStrip, TC_T);
+    const int bpr = kernel_blocks_per_sm(kr, Gm::kSmemRows, TR_T);
     // One column-strip launch and one row-block launch over the whole batch.  Cutting the batch
     // into L2-sized chunks (so that the intermediate stays in L2 between the two passes) measured
     // slower on every two-pass shape: the four-step kernels are bound by shared-memory latency,
@@ -89,21 +94,21 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
     const long long nb = batch;
     cudaError_t e;
     if (nb * (W / Gm::kTC) < 2LL * ctx.sm_count) {   // few arrays: smaller strips and row blocks
-      auto kcs = k_colstrip<H, W, Gm::kTCs, MODE>;
+      auto kcs = k_colstrip<H, W, Gm::kTCs, MODE, TC_T>;
       TileArgs ac{x, y, nb * (W / Gm::kTCs), nb * H, tab};
-      e = launch_tiles(kcs, Gm::kSmemStripS, kernel_blocks_per_sm(kcs, Gm::kSmemStripS), ac, ctx, st);
+      e = launch_tiles(kcs, Gm::kSmemStripS, kernel_blocks_per_sm(kcs, Gm::kSmemStripS, TC_T), ac, ctx, st, TC_T);
     } else {
       TileArgs ac{x, y, nb * (W / Gm::kTC), nb * H, tab};
-      e = launch_tiles(kc, Gm::kSmemStrip, bpc, ac, ctx, st);
+      e = launch_tiles(kc, Gm::kSmemStrip, bpc, ac, ctx, st, TC_T);
     }
     if (e != cudaSuccess) return e;
     if (nb * H / Gm::kRB < 2LL * ctx.sm_count) {
-      auto krs = k_full<H, W, Gm::kRBs, false, true, MODE>;
+      auto krs = k_full<H, W, Gm::kRBs, false, true, MODE, TR_T>;
       TileArgs ar{y, y, nb * H / Gm::kRBs, nb * H, tab};
-      e = launch_tiles(krs, Gm::kSmemRowsS, kernel_blocks_per_sm(krs, Gm::kSmemRowsS), ar, ctx, st);
+      e = launch_tiles(krs, Gm::kSmemRowsS, kernel_blocks_per_sm(krs, Gm::kSmemRowsS, TR_T), ar, ctx, st, TR_T);
     } else {
       TileArgs ar{y, y, nb * H / Gm::kRB, nb * H, tab};
-      e = launch_tiles(kr, Gm::kSmemRows, bpr, ar, ctx, st);
+      e = launch_tiles(kr, Gm::kSmemRows, bpr, ar, ctx, st, TR_T);
     }
     if (e != cudaSuccess) return e;
     return cudaSuccess;

@@ -146,16 +146,16 @@ __device__ __forceinline__ void tile_load(const float* g, long long gp, int rows
 // A tile held in registers between its global load and its shared-memory store, so that the
 // next tile's loads are in flight while the current tile is transformed (ROWS x COLS floats,
 // row pitch P in shared memory; element i of the tile's float4 sequence goes to thread i % 256).
-template <int P, int ROWS, int COLS>
+template <int P, int ROWS, int COLS, int THREADS = kThreads>
 struct TileRegs {
   static constexpr int Q = COLS / 4;
-  static constexpr int N = (ROWS * Q + kThreads - 1) / kThreads;
+  static constexpr int N = (ROWS * Q + THREADS - 1) / THREADS;
   float4 v[N];
   __device__ __forceinline__ void load(const float* g, long long gp, int valid_rows) {
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-      const int i = threadIdx.x + k * kThreads;
-      if (ROWS * Q % kThreads == 0 || i < ROWS * Q) {
+      const int i = threadIdx.x + k * THREADS;
+      if (ROWS * Q % THREADS == 0 || i < ROWS * Q) {
         const int r = i / Q, c = (i % Q) * 4;
         v[k] = r < valid_rows ? __ldg(reinterpret_cast<const float4*>(g + r * gp + c))
                               : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -165,8 +165,8 @@ struct TileRegs {
   __device__ __forceinline__ void put(float* tile) const {
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-      const int i = threadIdx.x + k * kThreads;
-      if (ROWS * Q % kThreads == 0 || i < ROWS * Q) {
+      const int i = threadIdx.x + k * THREADS;
+      if (ROWS * Q % THREADS == 0 || i < ROWS * Q) {
         const int r = i / Q, c = (i % Q) * 4;
         float* d = tile + r * P + c;
         if constexpr (P % 4 == 0) {
@@ -223,10 +223,10 @@ __device__ __forceinline__ void run_lines(float* tile, int nlines, int es, const
 
 // Full-width tiles: TR consecutive rows (of width W) of the batch viewed as a (B*H) x W
 // matrix.  With DO_COL the tile holds TR/H whole arrays.
-template <int H, int W, int TR, bool DO_COL, bool DO_ROW, int MODE>
-__global__ void __launch_bounds__(kThreads) k_full(TileArgs a) {
+template <int H, int W, int TR, bool DO_COL, bool DO_ROW, int MODE, int THREADS = kThreads>
+__global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
   constexpr int P = DO_COL ? pitch_of(H, W, true) : rowblock_pitch(W);
-  constexpr int XB = kWarps * cmax(DO_COL ? ExchangeFloats<H>::value : 0, DO_ROW ? ExchangeFloats<W>::value : 0);
+  constexpr int XB = (THREADS / 32) * cmax(DO_COL ? ExchangeFloats<H>::value : 0, DO_ROW ? ExchangeFloats<W>::value : 0);
   extern __shared__ float smem[];
   float* tile = smem;
   float* xbuf = smem + round4(TR * P);
@@ -244,9 +244,10 @@ __global__ void __launch_bounds__(kThreads) k_full(TileArgs a) {
   // 16384-float tiles whose rows are the long axis (64x256, 32x512, 16x1024, 64 prefetch floats a
   // thread) and row passes of 256..1024-point lines load with cp.async instead: measured +3-27%
   // and +1-11% over the register prefetch there.  Short-line tiles keep their occupancy.
-  constexpr bool kPrefetch = DO_COL ? DO_ROW && (H >= 128 || W >= 128) && !(W >= 256 && TR * W >= 16384)
-                                    : (DO_ROW && W == 128);
-  TileRegs<P, kPrefetch ? TR : 4, kPrefetch ? W : 4> next;
+  constexpr bool kPrefetch = THREADS == kThreads &&
+                             (DO_COL ? DO_ROW && (H >= 128 || W >= 128) && !(W >= 256 && TR * W >= 16384)
+                                     : (DO_ROW && W == 128));
+  TileRegs<P, kPrefetch ? TR : 4, kPrefetch ? W : 4, THREADS> next;
   if (kPrefetch && blockIdx.x < a.ntiles) next.load(a.x + blockIdx.x * (long long)TR * W, W, rows_of(blockIdx.x));
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const int rows = rows_of(t);
@@ -274,19 +275,19 @@ __global__ void __launch_bounds__(kThreads) k_full(TileArgs a) {
 }
 
 // Column strips: H rows x TC columns of one array (row pitch W in global memory).
-template <int H, int W, int TC, int MODE>
-__global__ void __launch_bounds__(kThreads) k_colstrip(TileArgs a) {
+template <int H, int W, int TC, int MODE, int THREADS = kThreads>
+__global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
   constexpr int P = strip_pitch(H, TC);
   constexpr int STRIPS = W / TC;
   extern __shared__ float smem[];
   float* tile = smem;
   float* xbuf = smem + round4(H * P);
-  const FourStepTables tcol = stage_tables<H>(a.tab.col, xbuf + round4(kWarps * ExchangeFloats<H>::value));
+  const FourStepTables tcol = stage_tables<H>(a.tab.col, xbuf + round4((THREADS / 32) * ExchangeFloats<H>::value));
   // Strips of 128- and 256-point columns prefetch the next strip into registers during the
   // transform; longer columns keep their occupancy.
-  constexpr bool kPrefetch = H == 128 || H == 256;
+  constexpr bool kPrefetch = THREADS == kThreads && (H == 128 || H == 256);
   auto src = [&](long long t) { return a.x + (t / STRIPS) * (long long)H * W + (t % STRIPS) * TC; };
-  TileRegs<P, kPrefetch ? H : 4, kPrefetch ? TC : 4> next;
+  TileRegs<P, kPrefetch ? H : 4, kPrefetch ? TC : 4, THREADS> next;
   if (kPrefetch && blockIdx.x < a.ntiles) next.load(src(blockIdx.x), W, H);
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const long long arr = t / STRIPS;
