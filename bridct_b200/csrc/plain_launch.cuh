@@ -72,10 +72,15 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
                           (W == 128 && H <= 32 && MODE != LM_RT);
     constexpr int TR = kBig ? Gm::kTRBig : Gm::kTR;
     constexpr int smem = kBig ? Gm::kSmemFullBig : Gm::kSmemFull;
-    auto k = k_full<H, W, TR, true, true, MODE>;
-    const int bps = kernel_blocks_per_sm(k, smem);
+    // 128 x 128 tiles (both passes 128-point register lines, 255 registers) run 128-thread CTAs:
+    // every warp has a line and two CTAs share an SM (+31..64% over one 256-thread CTA with
+    // register prefetch, in which half the warps have no line).  Tiles that mix 128-point register
+    // lines with many short lines measured 5..13% slower that way.
+    constexpr int T = H == 128 && W == 128 ? 128 : kThreads;
+    auto k = k_full<H, W, TR, true, true, MODE, T>;
+    const int bps = kernel_blocks_per_sm(k, smem, T);
     TileArgs a{x, y, (batch * H + TR - 1) / TR, batch * H, tab};
-    return launch_tiles(k, smem, bps, a, ctx, st);
+    return launch_tiles(k, smem, bps, a, ctx, st, T);
   } else {
     // Round trips of 128-point register lines run 128-thread CTAs without register prefetch:
     // every warp has a line and two CTAs share an SM, which measured +8..13% over one 256-thread
