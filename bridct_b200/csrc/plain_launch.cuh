@@ -72,11 +72,12 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
                           (W == 128 && H <= 32 && MODE != LM_RT);
     constexpr int TR = kBig ? Gm::kTRBig : Gm::kTR;
     constexpr int smem = kBig ? Gm::kSmemFullBig : Gm::kSmemFull;
-    // 128 x 128 tiles (both passes 128-point register lines, 255 registers) run 128-thread CTAs:
-    // every warp has a line and two CTAs share an SM (+31..64% over one 256-thread CTA with
-    // register prefetch, in which half the warps have no line).  Tiles that mix 128-point register
-    // lines with many short lines measured 5..13% slower that way.
-    constexpr int T = H == 128 && W == 128 ? 128 : kThreads;
+    // 128 x 128 tiles (both passes 128-point register lines, 255 registers) and round trips of
+    // tiles with a 128-point axis run 128-thread CTAs: two CTAs share an SM (128 x 128 +31..64%
+    // over one 256-thread CTA with register prefetch, in which half the warps have no line; the
+    // round trips +3..30% together with their register lines).  Forward / inverse tiles that mix
+    // 128-point register lines with many short lines measured 5..13% slower that way.
+    constexpr int T = (H == 128 && W == 128) || (MODE == LM_RT && (H == 128 || W == 128)) ? 128 : kThreads;
     auto k = k_full<H, W, TR, true, true, MODE, T>;
     const int bps = kernel_blocks_per_sm(k, smem, T);
     TileArgs a{x, y, (batch * H + TR - 1) / TR, batch * H, tab};

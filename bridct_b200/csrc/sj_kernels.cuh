@@ -23,10 +23,11 @@ constexpr int kTileFloats = 8192;   // target floats per CTA tile for small arra
 // Longest line run as one thread's straight-line program for a pass of N-point lines whose
 // array has `other` points on the other axis.  128-point register lines (168 registers, no
 // spills) measured +12-59% over the four-step on 128x128, the two-pass shapes and forward /
-// inverse tiles with a short other axis, and -6..-28% on round trips of tiles with a short
-// other axis and on tiles mixing them with 64-point lines: those keep the four-step.
+// inverse tiles with a short other axis, and -6..-28% on tiles mixing them with 64-point lines
+// in forward / inverse.  Round trips of tiles with a 128-point axis take them too, in 128-thread
+// CTAs (launch_plain): +3..30% over the four-step (128x8 alone -3%).
 __host__ __device__ constexpr int reg_line_max(int N, int other, int mode, bool two_pass) {
-  return N == 128 && (two_pass || other >= 128 || (mode != LM_RT && other <= 32)) ? 128 : 64;
+  return N == 128 && (two_pass || other >= 128 || mode == LM_RT || other <= 32) ? 128 : 64;
 }
 
 struct LineTables {
