@@ -82,6 +82,15 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
     const int bps = kernel_blocks_per_sm(k, smem, T);
     TileArgs a{x, y, (batch * H + TR - 1) / TR, batch * H, tab};
     return launch_tiles(k, smem, bps, a, ctx, st, T);
+  } else if constexpr (H * W == 32768 && (MODE == LM_INV || H == 1024 || H == 64 || (H == 32 && MODE == LM_FWD))) {
+    // Whole 32768-float arrays as tiles (one CTA per SM, both passes in shared memory) instead of
+    // the two passes, where that measured faster: every inverse (+5..21%), forward of 1024 x 32,
+    // 32 x 1024 and 64 x 512 (+2..14%), round trips of 1024 x 32 and 64 x 512 (+2..6%); round
+    // trips of 128 x 256 and 256 x 128 measured 30% slower.
+    auto k = k_full<H, W, H, true, true, MODE>;
+    const int bps = kernel_blocks_per_sm(k, Gm::kSmemWhole);
+    TileArgs a{x, y, batch, batch * H, tab};
+    return launch_tiles(k, Gm::kSmemWhole, bps, a, ctx, st);
   } else {
     // Round trips of 128-point register lines run 128-thread CTAs without register prefetch:
     // every warp has a line and two CTAs share an SM, which measured +8..13% over one 256-thread

@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
   // 16384-float tiles whose rows are the long axis (64x256, 32x512, 16x1024, 64 prefetch floats a
   // thread) and row passes of 256..1024-point lines load with cp.async instead: measured +3-27%
   // and +1-11% over the register prefetch there.  Short-line tiles keep their occupancy.
-  constexpr bool kPrefetch = THREADS == kThreads &&
+  constexpr bool kPrefetch = THREADS == kThreads && TR * W <= 16384 &&
                              (DO_COL ? DO_ROW && (H >= 128 || W >= 128) && !(W >= 256 && TR * W >= 16384)
                                      : (DO_ROW && W == 128));
   TileRegs<P, kPrefetch ? TR : 4, kPrefetch ? W : 4, THREADS> next;
@@ -336,6 +336,9 @@ struct Geometry {
   static constexpr int kArraysBig = pick_arrays(2 * kTileFloats);
   static constexpr int kTRBig = kTile ? kArraysBig * H : 1;
   static constexpr int kSmemFullBig = full_smem(kArraysBig);
+  // One whole array of 32768 floats per tile (one CTA per SM, 178-184 KB of shared memory), for
+  // the two-pass shapes and modes where it measured faster than the two passes (launch_plain).
+  static constexpr int kSmemWhole = full_smem(1);
   // 2-pass class
   static constexpr int strip_smem(int tc) {
     return (round4(H * strip_pitch(H, tc)) + round4(kWarps * ExchangeFloats<H>::value) + TableFloats<H>::value) * 4;
