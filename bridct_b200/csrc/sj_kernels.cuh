@@ -10,6 +10,8 @@
 //                           place), one launch each over the whole batch.  The intermediate
 //                           lives in y (the reference's rect route does the same pair of
 //                           passes, vertical then bands, src/generated/rect.c:5-23).
+//                           A 32768-float array runs as one whole-array tile instead (one CTA
+//                           per SM) in the modes where that measured faster (plain_launch.cuh).
 // Shared-memory rows use an odd pitch (w + 1 floats) so that a thread-per-row line walk and a
 // thread-per-column line walk are both bank-conflict free.
 #pragma once
