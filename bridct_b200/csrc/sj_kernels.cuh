@@ -12,8 +12,8 @@
 //                           passes, vertical then bands, src/generated/rect.c:5-23).
 //                           A 32768-float array runs as one whole-array tile instead (one CTA
 //                           per SM) in the modes where that measured faster (plain_launch.cuh).
-// Shared-memory rows use an odd pitch (w + 1 floats) so that a thread-per-row line walk and a
-// thread-per-column line walk are both bank-conflict free.
+// Shared-memory rows are padded (pitch_of, strip_pitch, rowblock_pitch) so that the line walks
+// of both passes stay free of most bank conflicts.
 #pragma once
 #include "sj_lines.cuh"
 
@@ -114,7 +114,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Moves rows x cols floats between global memory (row pitch gp) and the tile (pitch P).  Rows
 // from valid_rows on are zero-filled.  With an even pitch the load is asynchronous (cp.async of 16
-// or 8 bytes): a thread has its whole share of the tile in flight at once, which measured +4..23%
+// or 8 bytes): a thread has its whole share of the tile in flight at once, which measured +4..22%
 // on tiles of short lines and +6..12% on 1024-point row passes.  An odd pitch (column passes of
 // 512- and 1024-point lines) would need four 4-byte copies per float4, which measured 6-14% slower
 // than the synchronous float4 load it keeps.
@@ -148,7 +148,8 @@ __device__ __forceinline__ void tile_load(const float* g, long long gp, int rows
 
 // A tile held in registers between its global load and its shared-memory store, so that the
 // next tile's loads are in flight while the current tile is transformed (ROWS x COLS floats,
-// row pitch P in shared memory; element i of the tile's float4 sequence goes to thread i % 256).
+// row pitch P in shared memory; element i of the tile's float4 sequence goes to thread
+// i % THREADS).
 template <int P, int ROWS, int COLS, int THREADS = kThreads>
 struct TileRegs {
   static constexpr int Q = COLS / 4;
@@ -246,7 +247,8 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
   // next tile into registers during the transform (measured +10-50% on such shapes).  Full
   // 16384-float tiles whose rows are the long axis (64x256, 32x512, 16x1024, 64 prefetch floats a
   // thread) and row passes of 256..1024-point lines load with cp.async instead: measured +3-27%
-  // and +1-11% over the register prefetch there.  Short-line tiles keep their occupancy.
+  // and +1-11% over the register prefetch there.  Short-line tiles keep their occupancy, and
+  // 128-thread CTAs and whole 32768-float tiles have no registers to spare for it.
   constexpr bool kPrefetch = THREADS == kThreads && TR * W <= 16384 &&
                              (DO_COL ? DO_ROW && (H >= 128 || W >= 128) && !(W >= 256 && TR * W >= 16384)
                                      : (DO_ROW && W == 128));
