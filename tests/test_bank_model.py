@@ -105,3 +105,11 @@ def test_paired_stage2_rounds_of_128_and_256_point_lines():
 def test_even_pitch_of_512_point_strips_costs_no_more_than_the_odd_one():
     # 32-column strips of 512-point lines use pitch 34 instead of 33 so that they load asynchronously
     assert four_step_wavefronts(16, 34, rows=False) <= four_step_wavefronts(16, 33, rows=False)
+
+
+def test_odd_pitch_of_1024_point_strips():
+    # 1024-point column strips keep the odd pitch tc + 1: with 32 lanes on one line, an even pitch
+    # puts pairs of gather lanes in one bank (tc + 2 counts about 22% more wavefronts)
+    for tc in (8, 16):
+        odd, even = four_step_wavefronts(32, tc + 1, rows=False), four_step_wavefronts(32, tc + 2, rows=False)
+        assert even > 1.2 * odd
