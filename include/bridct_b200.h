@@ -92,6 +92,9 @@ typedef struct {
 
 typedef struct bridct_ragged bridct_ragged;
 
+/* Fills the library default: units of up to 16384 floats and a look-ahead of 32 arrays (the
+ * fastest measured on a mixed batch of all 64 shapes, apart from look-ahead 64, which was 0.6%
+ * faster). */
 BRIDCT_API void bridct_ragged_default_tuning(bridct_ragged_tuning *tuning);
 /* Validates the items (supported shapes and modes, aligned, non-overlapping) and builds the
  * device work queue; NULL on error (see bridct_last_error). */
