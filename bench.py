@@ -9,13 +9,16 @@ Default workload: 262,144 independent 8x8 blocks of a 4096x4096 image (pixels un
 one forward transform of all blocks (one pass of the hot path over the batch).  Algorithmic
 traffic is 8 bytes per element (read 4, write 4).  Timed steps replay a CUDA graph of
 launches over rotating input/output buffer sets that together exceed the 126 MB L2 (two sets,
-256 MiB, on the default workload), timed with CUDA events on the launching stream; multi-GPU
-runs are independent replicas per GPU (the batch shards with no exchange step), timed as the
-max over ranks.  Tensor-core forms also report their FLOP rate against the measured tensor
-peak; the CPU baseline reports all host threads and one thread.
+256 MiB, on the default workload).  The timed region holds at least --blocks (21) consecutive
+blocks of --steps steps, with CUDA events between the blocks on the launching stream; the value
+is the median block, and the line carries the spread.  With N GPUs the job's batch is N copies
+of the workload's arrays, sharded by rank (no exchange step), timed as the max over ranks.
+Tensor-core forms also report their FLOP rate against the measured tensor peak; the CPU baseline
+reports all host threads and one thread.
 
-`e2e` is the same metric through the public C-ABI (bridct_plan_apply_batch) from pinned host
-buffers: every step copies the inputs host->device and the results device->host.
+`e2e` is the same metric through the public C-ABI (bridct_plan_apply_batch) from host buffers:
+every call copies the inputs host->device and the results device->host (median call; pinned
+buffers, and a `pageable` leg with NumPy arrays).
 `--impl reference` times the reference library (compiled from its sources into oracle/_ref)
 on the host cores with one plan per thread.
 """
@@ -356,13 +359,43 @@ def time_form(torch, lib, plan, form_id, xs, ys, batch, mode, steps, warmup, str
     return plan_of
 
 
+def time_blocks(torch, stream, replay, nblocks, dev):
+    """Device time (ms) of `nblocks` consecutive blocks, each one `replay()` of the K-step loop,
+    from CUDA events recorded between the blocks on the launching stream; the whole region is
+    bracketed by synchronizes (and barriers under torchrun).  Returns per-block ms, each the max
+    over ranks."""
+    from bridct_b200.dist import max_over_ranks
+
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(nblocks + 1)]
+    with torch.cuda.stream(stream):
+        evs[0].record(stream)
+        for i in range(nblocks):
+            replay()
+            evs[i + 1].record(stream)
+    evs[-1].synchronize()
+    torch.cuda.synchronize()
+    return max_over_ranks([evs[i].elapsed_time(evs[i + 1]) for i in range(nblocks)], dev)
+
+
+def block_count(probe_ms: float, min_blocks: int, target_s: float = 1.0) -> int:
+    """At least `min_blocks` blocks, and enough of them to fill about `target_s` of device time."""
+    return int(min(4000, max(min_blocks, np.ceil(target_s * 1e3 / max(probe_ms, 1e-3)))))
+
+
+def spread(ms):
+    return {"blocks": len(ms), "min_ms": min(ms), "median_ms": statistics.median(ms), "max_ms": max(ms)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None,
-                    help="timed steps (default 20000; 1000 for the ragged workload, whose per-array "
-                         "launch loop takes about 28 ms a step)")
+                    help="steps per timed block (default 200; 20 for the ragged workload, whose "
+                         "per-array launch loop takes about 28 ms a step)")
     ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--blocks", type=int, default=21,
+                    help="least number of timed blocks of --steps steps; the value is the median "
+                         "block (more blocks are timed when needed to fill about a second)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="blocks8")
     ap.add_argument("--form", default="auto")
@@ -375,7 +408,7 @@ def main():
                     help="use the first N arrays of the workload (repeated cyclically when N is larger)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 1000 if args.workload == "ragged" else 20000
+        args.steps = 20 if args.workload == "ragged" else 200
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus))
@@ -413,6 +446,10 @@ def main():
     xh = wl["x"]
     if args.batch:
         xh = np.ascontiguousarray(np.resize(xh, (args.batch,) + xh.shape[1:]))
+    # The job's batch is `world` copies of the workload's arrays; every rank transforms its own
+    # shard of it (shard_range: contiguous, sizes differ by at most one) and no collective touches
+    # the data, so the per-GPU work stays fixed as N grows (weak scaling).
+    xh, first = shard_of(xh, rank, world)
     b, h, w = xh.shape
     mode = wl["mode"]
     bytes_step = 8.0 * b * h * w
@@ -456,26 +493,29 @@ def main():
     timings = {}
     for name, fid in forms.items():
         graphs = time_form(torch, lib, plan, fid, xs, ys, b, mode, args.steps, args.warmup, stream)
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        start = torch.cuda.Event(enable_timing=True)
-        end = torch.cuda.Event(enable_timing=True)
+
+        def replay():
+            for g in graphs:
+                g.replay()
+
+        probe = time_blocks(torch, stream, replay, 1, dev)[0]
+        nblocks = block_count(probe, args.blocks)
         clk = Clocks(local)
         with clk:
-            with torch.cuda.stream(stream):
-                start.record(stream)
-                for g in graphs:
-                    g.replay()
-                end.record(stream)
-            end.synchronize()
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        ms = start.elapsed_time(end)
-        ms = max_over_ranks(ms, dev)
-        timings[name] = {"ms_total": ms, "ms_per_step": ms / args.steps, "clocks": clk.summary(),
-                         "gbs": bytes_step * args.steps * world / (ms * 1e-3) / 1e9}
+            warm_until = time.perf_counter() + 0.3      # untimed replays while the clocks settle
+            while time.perf_counter() < warm_until:
+                with torch.cuda.stream(stream):
+                    replay()
+                stream.synchronize()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            blocks = time_blocks(torch, stream, replay, nblocks, dev)
+            if world > 1:
+                dist.barrier()
+        ms = statistics.median(blocks)
+        timings[name] = {"ms_block": ms, "ms_per_step": ms / args.steps, "clocks": clk.summary(),
+                         "gbs": bytes_step * args.steps * world / (ms * 1e-3) / 1e9, "spread": spread(blocks)}
         del graphs
 
     # headline: the fastest form whose error meets the bound (2e-6, output-scaled max norm)
@@ -489,22 +529,34 @@ def main():
     if tfile.exists():
         traffic = json.loads(tfile.read_text()).get(f"{args.workload}:{head}")
 
-    # e2e through the public C-ABI with pinned host buffers
+    # e2e through the public C-ABI (bridct_plan_apply_batch) from host buffers: every call copies
+    # the inputs in and the results out; the median call of each leg is reported.
+    def e2e_leg(src, dst):
+        calls = max(21, min(200, args.steps))
+        for _ in range(2):
+            _lib.check(lib.bridct_plan_apply_batch(plan, mode, src, dst, b))
+        if world > 1:
+            dist.barrier()
+        per = []
+        for _ in range(calls):
+            t0 = time.perf_counter()
+            _lib.check(lib.bridct_plan_apply_batch(plan, mode, src, dst, b))
+            per.append(time.perf_counter() - t0)
+        per = max_over_ranks(per, dev)
+        med = statistics.median(per)
+        return {"value": bytes_step * world / med / 1e9, "unit": "GB/s", "ms_per_step": 1e3 * med,
+                "calls": calls}
+
     hin = torch.from_numpy(xh).pin_memory()
     hout = torch.empty_like(hin).pin_memory()
-    e2e_steps = max(3, min(50, args.steps))
-    for _ in range(2):
-        _lib.check(lib.bridct_plan_apply_batch(plan, mode, hin.data_ptr(), hout.data_ptr(), b))
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        _lib.check(lib.bridct_plan_apply_batch(plan, mode, hin.data_ptr(), hout.data_ptr(), b))
-    e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(e2e_s, dev)
-    e2e = {"value": bytes_step * e2e_steps * world / e2e_s / 1e9, "unit": "GB/s",
-           "h2d_bytes_per_step": int(4 * b * h * w), "d2h_bytes_per_step": int(4 * b * h * w),
-           "form": "sj", "ms_per_step": 1e3 * e2e_s / e2e_steps}
+    e2e = e2e_leg(hin.data_ptr(), hout.data_ptr())
+    e2e.update({"h2d_bytes_per_step": int(4 * b * h * w), "d2h_bytes_per_step": int(4 * b * h * w),
+                "form": "sj", "host_memory": "pinned"})
+    del hin, hout
+    pageable_out = np.empty_like(xh)
+    e2e["pageable"] = e2e_leg(xh.ctypes.data, pageable_out.ctypes.data)
+    e2e["pageable"]["host_memory"] = "pageable (NumPy arrays), staged through the plan's pinned slots"
+    del pageable_out
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -533,20 +585,27 @@ def main():
         "dtype": "f32" if head == "sj" else head.replace("tc_", "") + "/f32-acc",
         "data": "synthetic",
         "config": {"workload": wl["desc"], "arrays": b, "shape": [h, w], "mode": "forward",
-                   "form": head, "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "form": head, "parallelism": parallelism(world, b, first),
                    "l2": f"{sets} rotating input/output sets ({sets * 8 * b * h * w / 2**20:.0f} MiB) > L2",
-                   "timing": "CUDA events on the launch stream around CUDA-graph replays"},
+                   "timing": f"median of {timings[head]['spread']['blocks']} blocks of {args.steps} steps "
+                             "(CUDA-graph replays), CUDA events between blocks on the launch stream"},
         "pct_hbm_peak": 100.0 * achieved / pk["hbm_gbs"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"],
-                     "traffic": traffic, "algorithmic_bytes_per_launch": bytes_step},
+                     "traffic": traffic, "traffic_source": "ncu capture of this kernel and workload "
+                     "(dram__bytes_read.sum + dram__bytes_write.sum per launch), recorded in "
+                     "profiles/traffic.json; not measured in this run" if traffic else None,
+                     "algorithmic_bytes_per_launch": bytes_step},
+        "spread": timings[head]["spread"],
         "forms": {n: {**results[n], "gbs": timings[n]["gbs"], "ms_per_step": timings[n]["ms_per_step"],
+                      "spread": timings[n]["spread"],
                       "pct_hbm": 100 * timings[n]["gbs"] / world / pk["hbm_gbs"],
                       "tensor": tensor_rate(n, h, w, b * h * w / (timings[n]["ms_per_step"] * 1e-3), pk)}
                   for n in timings},
         "clocks": timings[head]["clocks"],
         "e2e": e2e,
-        "gpu_launches": int(args.steps * launches_per_step(h, w, b)),
+        "gpu_launches": int(args.steps * launches_per_step(head, h, w, b, mode)),
+        "gpu_launches_note": "launches in one timed block of `steps` steps (the value is the median block)",
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
@@ -586,26 +645,27 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
             for _ in range(max(3, args.warmup)):
                 fn(x, y, stream=stream.cuda_stream)
         stream.synchronize()
-        per_graph = 1 if name == "launch_loop" else min(args.steps, 16)
+        # one graph of the K steps (the launch loop: one step of 4096 launches, replayed K times)
+        per_graph = 1 if name == "launch_loop" else args.steps
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=stream):
             for _ in range(per_graph):
                 fn(x, y, stream=stream.cuda_stream)
-        reps = max(1, args.steps // per_graph)
+
+        def replay():
+            for _ in range(args.steps // per_graph):
+                g.replay()
+
+        probe = time_blocks(torch, stream, replay, 1, dev)[0]
+        nblocks = args.blocks if name == "launch_loop" else block_count(probe, args.blocks)
         if world > 1:
             dist.barrier()
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         clk = Clocks(local)
         with clk:
-            with torch.cuda.stream(stream):
-                start.record(stream)
-                for _ in range(reps):
-                    g.replay()
-                end.record(stream)
-            end.synchronize()
-        ms = max_over_ranks(start.elapsed_time(end), dev) / (reps * per_graph)
+            blocks = time_blocks(torch, stream, replay, nblocks, dev)
+        ms = statistics.median(blocks) / args.steps
         out[name] = {"ms_per_step": ms, "gbs": bytes_step * world / (ms * 1e-3) / 1e9, "clocks": clk.summary(),
-                     "steps": reps * per_graph}
+                     "steps": args.steps, "spread": spread(blocks)}
         del g
     assert not batch.timed_out()
     # accuracy on a sample of arrays
@@ -626,7 +686,10 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
             "data": "synthetic",
             "config": {"workload": wl["desc"], "arrays": len(wl["items"]), "floats": batch.span,
                        "units": batch.units, "tuning": tuning or "default",
-                       "timing": "CUDA events around CUDA-graph replays; inputs 1 GB > L2"},
+                       "parallelism": "single GPU" if world == 1 else f"dp{world}: every rank its own copy "
+                       "of the batch (no collective)",
+                       "timing": f"median of {head['spread']['blocks']} blocks of {args.steps} steps "
+                                 "(CUDA-graph replays), CUDA events on the launch stream; inputs 1 GB > L2"},
             "pct_hbm_peak": 100 * head["gbs"] / world / pk["hbm_gbs"],
             "forms": out, "max_rel_err_output_scaled_sample": worst,
             "speedup_vs_launch_loop": out["launch_loop"]["ms_per_step"] / head["ms_per_step"],
@@ -701,17 +764,16 @@ def run_image8(args, wl, rank, world, local, dist, torch):
             with torch.cuda.graph(g, stream=stream):
                 for i in range(args.steps):
                     torch_api.image_blocks8(xs[i % 2], 0, quant=q, out=ys[i % 2])
-            if world > 1:
-                dist.barrier()
-            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            clk = Clocks(local)
-            with clk:
-                start.record(stream)
-                g.replay()
-                end.record(stream)
-                end.synchronize()
-        ms = max_over_ranks(start.elapsed_time(end), dev) / args.steps
-        out[name] = {"ms_per_step": ms, "gbs": bytes_step * world / (ms * 1e-3) / 1e9, "clocks": clk.summary()}
+        probe = time_blocks(torch, stream, g.replay, 1, dev)[0]
+        nblocks = block_count(probe, args.blocks)
+        if world > 1:
+            dist.barrier()
+        clk = Clocks(local)
+        with clk:
+            blocks = time_blocks(torch, stream, g.replay, nblocks, dev)
+        ms = statistics.median(blocks) / args.steps
+        out[name] = {"ms_per_step": ms, "gbs": bytes_step * world / (ms * 1e-3) / 1e9, "clocks": clk.summary(),
+                     "spread": spread(blocks)}
         del g
     # accuracy on a band of block rows against float64 per block
     band = img[:512]
@@ -768,7 +830,8 @@ def run_image8(args, wl, rank, world, local, dist, torch):
         "config": {"workload": wl["desc"], "shape": [h, w], "mode": "forward", "form": "sj",
                    "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": "2 rotating input/output images (256 MiB) > L2",
-                   "timing": "CUDA events on the launch stream around CUDA-graph replays"},
+                   "timing": f"median of {head['spread']['blocks']} blocks of {args.steps} steps "
+                             "(CUDA-graph replays), CUDA events on the launch stream"},
         "pct_hbm_peak": 100.0 * achieved / pk["hbm_gbs"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"], "traffic": None,
@@ -777,11 +840,38 @@ def run_image8(args, wl, rank, world, local, dist, torch):
         "gpu_launches": args.steps, "cpu_baseline": cpu}))
 
 
-def launches_per_step(h: int, w: int, b: int) -> int:
-    if h * w <= 16384:
+def launches_per_step(form: str, h: int, w: int, b: int, mode: int) -> int:
+    """Kernel launches of one step of a form (the plain form: one for tiles and whole 32768-float
+    arrays, two for the two passes; tensor-core forms: one Kronecker or fused launch, two passes
+    per 1 GB chunk, or the FP8 form's quantize/pass/refine sequence)."""
+    e = h * w
+    if form == "sj":
+        whole = e == 32768 and (mode == 1 or h in (1024, 64) or (h == 32 and mode == 0))
+        return 1 if e <= 16384 or whole else 2
+    chunks = int(np.ceil(b * e * 4 / (1 << 30)))
+    if form == "tc_fp8":
+        return 12 * int(np.ceil(b * e * 4 / (256 << 20)))
+    if (h, w) == (8, 8) or (form == "tc_bf16x3" and (h, w) == (64, 64)):
         return 1
-    chunk = max(1, (126 * 2**20 // 4) // (4 * h * w))
-    return 2 * int(np.ceil(b / chunk))
+    return 2 * chunks
+
+
+def shard_of(x, rank: int, world: int):
+    """Rank's shard of a job batch made of `world` copies of the arrays in x: (arrays, first)."""
+    from bridct_b200.dist import shard_range
+
+    b = x.shape[0]
+    first, count = shard_range(b * world, rank, world)
+    if world == 1:
+        return x, 0
+    return np.ascontiguousarray(x[np.arange(first, first + count) % b]), first
+
+
+def parallelism(world: int, b: int, first: int) -> str:
+    if world == 1:
+        return "single GPU"
+    return (f"dp{world}: a batch of {world} x {b} arrays sharded by rank (contiguous shards of {b} arrays, "
+            "no collective on the data; timing is the max over ranks)")
 
 
 if __name__ == "__main__":

@@ -54,6 +54,7 @@ def lib() -> C.CDLL:
     _sig(L, "bridct_last_error", C.c_char_p, [])
     _sig(L, "bridct_plan_gpu_route", C.c_char_p, [vp])
     _sig(L, "bridct_plan_apply_batch", C.c_int, [vp, C.c_int, vp, vp, C.c_size_t])
+    _sig(L, "bridct_plan_roundtrip_batch", C.c_int, [vp, vp, vp, C.c_size_t])
     _sig(L, "bridct_plan_apply_device", C.c_int, [vp, C.c_int, vp, vp, C.c_size_t, vp])
     _sig(L, "bridct_plan_apply_form_device", C.c_int, [vp, C.c_int, C.c_int, vp, vp, C.c_size_t, vp])
     _sig(L, "bridct_plan_synchronize", C.c_int, [vp])
@@ -74,9 +75,13 @@ EXTRA_SIGNATURES = [
     ("bridct_ragged_apply_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("bridct_ragged_apply_loop_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("bridct_ragged_timeout_flag", C.c_int, [C.c_void_p]),
+    ("bridct_ragged_set_wait_limit", C.c_int, [C.c_void_p, C.c_uint]),
     ("bridct_device_timeout_flag", C.c_int, [C.c_int]),
     ("bridct_ragged_apply_noalloc", C.c_int, [C.POINTER(RaggedItem), C.c_size_t, C.c_void_p, C.c_void_p,
                                               C.c_void_p]),
+    ("bridct_plan_form_workspace_bytes", C.c_size_t, [C.c_void_p, C.c_int, C.c_size_t]),
+    ("bridct_plan_apply_form_device_ws", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                                   C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("bridct_image_blocks8_device", C.c_int, [C.c_int, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_int,
                                               C.c_int, C.c_void_p, C.c_void_p]),
 ]

@@ -241,7 +241,7 @@ BRIDCT_API int bridct_supported(int height, int width) {
 BRIDCT_API void bridct_plan_destroy(bridct_plan* plan) {
   if (!plan) return;
   int prev = -1;
-  cudaGetDevice(&prev);
+  if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
   cudaSetDevice(plan->device);
   if (plan->stream) cudaStreamSynchronize(plan->stream);
   for (int i = 0; i < 3; ++i)
@@ -305,7 +305,8 @@ BRIDCT_API int bridct_plan_apply(bridct_plan* plan, enum bridct_mode mode, const
   if (!plan || !input || !output || (unsigned)mode > BRIDCT_ROUNDTRIP) return BRIDCT_INVALID_ARGUMENT;
   const size_t bytes = plan->elements * sizeof(float);
   if (ranges_overlap((uintptr_t)input, bytes, (uintptr_t)output, bytes)) return BRIDCT_OVERLAPPING_BUFFERS;
-  cudaSetDevice(plan->device);
+  DeviceGuard guard(plan->device);
+  if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(plan device)");
   bool pin_in = false, pin_out = false;
   const float* dx = (const float*)device_address(input, &pin_in);
   float* dy = (float*)device_address(output, &pin_out);
@@ -357,6 +358,9 @@ BRIDCT_API int bridct_plan_apply_device(bridct_plan* plan, enum bridct_mode mode
   const size_t bytes = plan->elements * sizeof(float) * batch;
   if (ranges_overlap((uintptr_t)input, bytes, (uintptr_t)output, bytes)) return BRIDCT_OVERLAPPING_BUFFERS;
   if (((uintptr_t)input | (uintptr_t)output) % 16) return BRIDCT_BAD_ALIGNMENT;
+  // The launch runs on the plan's device (its tables live there) whatever device is current.
+  DeviceGuard guard(plan->device);
+  if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(plan device)");
   // NULL is the CUDA default stream, as everywhere in CUDA (torch's default stream too).
   return launch_plain_form(plan, mode, input, output, (long long)batch, (cudaStream_t)stream);
 }
@@ -374,7 +378,8 @@ BRIDCT_API int bridct_plan_apply_batch(bridct_plan* plan, enum bridct_mode mode,
   const size_t per = plan->elements * sizeof(float);
   const size_t bytes = per * batch;
   if (ranges_overlap((uintptr_t)input, bytes, (uintptr_t)output, bytes)) return BRIDCT_OVERLAPPING_BUFFERS;
-  cudaSetDevice(plan->device);
+  DeviceGuard guard(plan->device);
+  if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(plan device)");
   bool pin_in = false, pin_out = false;
   const float* dx = (const float*)device_address(input, &pin_in);
   float* dy = (float*)device_address(output, &pin_out);
@@ -385,6 +390,18 @@ BRIDCT_API int bridct_plan_apply_batch(bridct_plan* plan, enum bridct_mode mode,
     return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "bridct_plan_apply_batch");
   }
   return host_batch_pipeline(plan, mode, input, output, batch, dx, dy, pin_in, pin_out);
+}
+
+BRIDCT_API int bridct_plan_roundtrip_batch(bridct_plan* plan, const float* input, float* output, size_t batch) {
+  if (!plan || !input || !output || batch == 0) return BRIDCT_INVALID_ARGUMENT;
+  const size_t bytes = plan->elements * sizeof(float) * batch;
+  if (ranges_overlap((uintptr_t)input, bytes, (uintptr_t)output, bytes)) return BRIDCT_OVERLAPPING_BUFFERS;
+  DeviceGuard guard(plan->device);
+  if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(plan device)");
+  bool pin_in = false, pin_out = false;
+  const float* dx = (const float*)device_address(input, &pin_in);
+  float* dy = (float*)device_address(output, &pin_out);
+  return host_batch_pipeline(plan, kModeSpectrumRT, input, output, batch, dx, dy, pin_in, pin_out);
 }
 
 BRIDCT_API size_t bridct_workspace_floats(int n) {
@@ -418,5 +435,32 @@ extern "C" BRIDCT_API int bridct_plan_apply_form_device(bridct_plan* plan, enum 
                                                         enum bridct_form form, const float* input,
                                                         float* output, size_t batch, void* stream) {
   if (form == BRIDCT_FORM_SJ) return bridct_plan_apply_device(plan, mode, input, output, batch, stream);
-  return bridct::apply_tc_form(plan, (int)mode, (int)form, input, output, batch, stream);
+  if (!plan) return BRIDCT_INVALID_ARGUMENT;
+  bridct::DeviceGuard guard(plan->device);
+  if (guard.status != cudaSuccess) return bridct::cuda_fail(guard.status, "cudaSetDevice(plan device)");
+  return bridct::apply_tc_form(plan, (int)mode, (int)form, input, output, batch, stream, nullptr, 0);
+}
+
+extern "C" BRIDCT_API size_t bridct_plan_form_workspace_bytes(const bridct_plan* plan, enum bridct_form form,
+                                                              size_t batch) {
+  if (!plan || batch == 0 || form == BRIDCT_FORM_SJ) return 0;
+  return bridct::tc_workspace_bytes(plan, (int)form, batch);
+}
+
+extern "C" BRIDCT_API int bridct_plan_apply_form_device_ws(bridct_plan* plan, enum bridct_mode mode,
+                                                           enum bridct_form form, const float* input,
+                                                           float* output, size_t batch, void* workspace,
+                                                           size_t workspace_bytes, void* stream) {
+  if (form == BRIDCT_FORM_SJ) return bridct_plan_apply_device(plan, mode, input, output, batch, stream);
+  if (!plan) return BRIDCT_INVALID_ARGUMENT;
+  const size_t need = bridct::tc_workspace_bytes(plan, (int)form, batch);
+  if (need && !workspace) return BRIDCT_INVALID_ARGUMENT;
+  if (workspace_bytes < need) return BRIDCT_WORKSPACE_TOO_SMALL;
+  if ((uintptr_t)workspace % 16) return BRIDCT_BAD_ALIGNMENT;
+  bridct::DeviceGuard guard(plan->device);
+  if (guard.status != cudaSuccess) return bridct::cuda_fail(guard.status, "cudaSetDevice(plan device)");
+  // a form that needs no scratch gets a non-NULL marker so that the plan's own scratch is not used
+  static char unused;
+  return bridct::apply_tc_form(plan, (int)mode, (int)form, input, output, batch, stream,
+                               need ? workspace : static_cast<void*>(&unused), workspace_bytes);
 }

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -36,6 +37,29 @@ int kernel_setup(const void* kernel, int smem, int threads);
 int current_device(int* dev);
 const void* device_address(const void* p, bool* pinned);
 
+// Makes `device` current for the guard's scope and gives the caller's current device back at
+// scope exit, so an entry point never leaves another device current than the one it found.
+struct DeviceGuard {
+  int prev = -1;
+  cudaError_t status = cudaSuccess;
+  explicit DeviceGuard(int device) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) {
+      cudaGetLastError();
+      cur = -1;
+    }
+    if (cur != device) {
+      status = cudaSetDevice(device);
+      prev = cur;
+    }
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 }  // namespace bridct
 
 struct bridct_plan {
@@ -56,12 +80,17 @@ struct bridct_plan {
   float* d_batch = nullptr;    // slots x (in, out) x chunk
   float* pin_batch = nullptr;  // slots x (in, out) x chunk, pageable callers only
   size_t chunk = 0;            // arrays per pipeline chunk
-  // precision-form scratch (allocated on first use of a tensor-core form)
+  // precision-form scratch (allocated on first use of a tensor-core form that is not given a
+  // caller workspace); tc_mu serializes its (re)allocation
   void* tc_mem = nullptr;
   size_t tc_bytes = 0;
+  std::mutex tc_mu;
 };
 
 namespace bridct {
+// Pipeline-only mode: forward then inverse with the float32 spectrum materialized on the device
+// (bitwise the composition of a FORWARD and an INVERSE call).
+constexpr int kModeSpectrumRT = 3;
 int launch_plain_form(const bridct_plan* p, int mode, const float* x, float* y, long long batch,
                       cudaStream_t st);
 int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, size_t batch,
@@ -72,6 +101,9 @@ void release_plan_extras(bridct_plan* p);
 
 namespace bridct {
 // Tensor-core precision forms (tc_forms.cu).
+// workspace: caller-owned scratch of ws_bytes (NULL: the plan's own scratch).
 int apply_tc_form(bridct_plan* p, int mode, int form, const float* x, float* y, size_t batch,
-                  void* stream);
+                  void* stream, void* workspace, size_t ws_bytes);
+// Scratch bytes a tensor-core form needs for `batch` arrays of the plan's shape (0: none).
+size_t tc_workspace_bytes(const bridct_plan* p, int form, size_t batch);
 }  // namespace bridct

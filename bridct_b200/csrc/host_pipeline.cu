@@ -22,7 +22,8 @@ static int ensure_batch_staging(bridct_plan* p, bool need_pinned) {
   if (!p->d_batch) {
     size_t c = kChunkBytes / per;
     p->chunk = c ? c : 1;
-    cudaError_t e = cudaMalloc((void**)&p->d_batch, 2 * kSlots * p->chunk * per);
+    // per slot: input, output and (materialized round trips) the float32 spectrum
+    cudaError_t e = cudaMalloc((void**)&p->d_batch, 3 * kSlots * p->chunk * per);
     if (e != cudaSuccess) return cuda_fail(e, "batch staging");
     for (int i = 0; i < 3; ++i) {
       e = cudaStreamCreateWithFlags(&p->aux[i], cudaStreamNonBlocking);
@@ -77,8 +78,9 @@ int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, s
   for (size_t na : sizes) {
     const int slot = (int)(ci % kSlots);
     const size_t off = a0 * per, nbytes = na * per * sizeof(float);
-    float* sx = p->d_batch + (size_t)slot * 2 * cf;
+    float* sx = p->d_batch + (size_t)slot * 3 * cf;
     float* sy = sx + cf;
+    float* sz = sy + cf;
     float* px = p->pin_batch ? p->pin_batch + (size_t)slot * 2 * cf : nullptr;
     float* py = px ? px + cf : nullptr;
     if (pending[slot]) {        // the host copies the slot's previous output out of pinned staging
@@ -117,7 +119,12 @@ int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, s
       e = cudaStreamWaitEvent(ks, ev_out[slot], 0);     // the slot's last copy out has read sy
       if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");
     }
-    s = launch_plain_form(p, mode, kx, ky, (long long)na, ks);
+    if (mode == kModeSpectrumRT) {   // forward into the slot's spectrum, inverse out of it
+      s = launch_plain_form(p, BRIDCT_FORWARD, kx, sz, (long long)na, ks);
+      if (!s) s = launch_plain_form(p, BRIDCT_INVERSE, sz, ky, (long long)na, ks);
+    } else {
+      s = launch_plain_form(p, mode, kx, ky, (long long)na, ks);
+    }
     if (s) return s;
     e = cudaEventRecord(ev_k[slot], ks);
     if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");

@@ -24,6 +24,7 @@ struct bridct_ragged {
   int* d_err = nullptr;
   size_t span = 0;                      // floats covered by the batch (max offset + size)
   int grid = 0;
+  unsigned spin_limit = bridct::kRaggedSpin;
   bridct_ragged_tuning tuning{};
   std::map<int, bridct_plan*> plans;    // per-array launch loop: one plan per shape
 };
@@ -217,6 +218,8 @@ BRIDCT_API int bridct_ragged_apply_device(bridct_ragged* r, const float* x, floa
   const uintptr_t a = (uintptr_t)x, b = (uintptr_t)y;
   if ((a <= b ? b - a : a - b) < bytes) return BRIDCT_OVERLAPPING_BUFFERS;
   if ((a | b) % 16) return BRIDCT_BAD_ALIGNMENT;
+  DeviceGuard guard(r->device);
+  if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(batch device)");
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e = cudaMemsetAsync(r->d_counters, 0, (r->items.size() + 1) * sizeof(unsigned int), st);
   if (e != cudaSuccess) return cuda_fail(e, "ragged reset");
@@ -229,14 +232,22 @@ BRIDCT_API int bridct_ragged_apply_device(bridct_ragged* r, const float* x, floa
   args.next = r->d_counters;
   args.done = r->d_counters + 1;
   args.err = r->d_err;
+  args.spin_limit = r->spin_limit;
   for (int i = 0; i < 4; ++i) args.tab[i] = r->dev->fourstep[i];
   k_ragged<<<r->grid, kRaggedThreads, kRaggedSmem, st>>>(args);
   e = cudaGetLastError();
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_ragged launch");
 }
 
+BRIDCT_API int bridct_ragged_set_wait_limit(bridct_ragged* r, unsigned polls) {
+  if (!r) return BRIDCT_INVALID_ARGUMENT;
+  r->spin_limit = polls;
+  return BRIDCT_OK;
+}
+
 BRIDCT_API int bridct_ragged_timeout_flag(bridct_ragged* r) {
   if (!r) return 0;
+  DeviceGuard guard(r->device);
   int v = 0;
   cudaMemcpy(&v, r->d_err, sizeof(int), cudaMemcpyDeviceToHost);
   if (v) cudaMemset(r->d_err, 0, sizeof(int));
@@ -249,6 +260,8 @@ BRIDCT_API int bridct_ragged_apply_loop_device(bridct_ragged* r, const float* x,
   const uintptr_t a = (uintptr_t)x, b = (uintptr_t)y;
   if ((a <= b ? b - a : a - b) < bytes) return BRIDCT_OVERLAPPING_BUFFERS;
   if ((a | b) % 16) return BRIDCT_BAD_ALIGNMENT;
+  DeviceGuard guard(r->device);
+  if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(batch device)");
   // one launch per array, grouped by shape so consecutive launches reuse kernels
   std::vector<int> order(r->items.size());
   for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
@@ -411,7 +424,10 @@ extern "C" BRIDCT_API int bridct_ragged_apply_noalloc(const bridct_ragged_item* 
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-  if (dev < 0 || dev >= 64) return BRIDCT_INVALID_ARGUMENT;
+  if (dev < 0 || dev >= 64) {
+    set_error("bridct_ragged_apply_noalloc: device index beyond 63");
+    return BRIDCT_INVALID_ARGUMENT;
+  }
   if (!g_na_tables) {
     for (int i = 0; i < 4; ++i) fill_fourstep_tables(128 << i, g_na_tw + na_segment(i), g_na_post + na_segment(i));
     g_na_tables = true;
@@ -449,6 +465,7 @@ extern "C" BRIDCT_API int bridct_ragged_apply_noalloc(const bridct_ragged_item* 
   args.next = reinterpret_cast<unsigned int*>(base + NaOff::counters);
   args.done = args.next + 1;
   args.err = reinterpret_cast<int*>(base + NaOff::err);
+  args.spin_limit = kRaggedSpin;
   for (int i = 0; i < 4; ++i) {
     args.tab[i].tw = reinterpret_cast<const float2*>(base + NaOff::tw) + na_segment(i);
     args.tab[i].post = reinterpret_cast<const float4*>(base + NaOff::post) + na_segment(i);

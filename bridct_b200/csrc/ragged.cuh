@@ -41,6 +41,7 @@ struct RaggedArgs {
   unsigned int* next;       // queue head (zeroed before the launch)
   unsigned int* done;       // finished column strips per array (zeroed before the launch)
   int* err;
+  unsigned spin_limit;      // polls of a row block's dependency wait before it gives up
   FourStepTables tab[4];    // N = 128, 256, 512, 1024
 };
 
@@ -184,7 +185,7 @@ __global__ void __launch_bounds__(kRaggedThreads, 2) k_ragged(RaggedArgs a) {
     } else {
       if (threadIdx.x == 0) {
         int ok = 0;
-        for (unsigned i = 0; i < kRaggedSpin; ++i) {
+        for (unsigned i = 0; i < a.spin_limit; ++i) {
           if (atomicAdd(a.done + unit.array, 0u) >= (unsigned)arr.nstrips) {
             ok = 1;
             break;

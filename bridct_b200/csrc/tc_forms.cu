@@ -441,25 +441,48 @@ int fp8_refined(const bridct_plan* p, bool inverse, const float* src, float* dst
   return ce == cudaSuccess ? BRIDCT_OK : cuda_fail(ce, "FP8 refinement");
 }
 
-int apply_fp8(bridct_plan* p, int mode, const float* x, float* y, size_t batch, cudaStream_t st, TcDevice* d) {
-  const size_t elems = p->elements;
-  // Chunks of 256 MB: the twelve launches of a refined transform dominate smaller chunks (2048
-  // arrays of 256x256, same outputs: 16 MB 304 GB/s, 32 MB 344, 64 MB 352-366, 256 MB 382,
-  // 1 GB 389); the scratch needs about 17 bytes per element of a chunk.
+// Arrays per chunk of the FP8 form.  Chunks of 256 MB: the twelve launches of a refined
+// transform dominate smaller chunks (2048 arrays of 256x256, same outputs: 16 MB 304 GB/s,
+// 32 MB 344, 64 MB 352-366, 256 MB 382, 1 GB 389); the scratch needs about 17 bytes per element
+// of a chunk.
+size_t fp8_chunk(size_t elems, size_t batch, size_t* bytes) {
   size_t chunk = (size_t(256) << 20) / (elems * sizeof(float));
   if (chunk < 1) chunk = 1;
   if (chunk > batch) chunk = batch;
   const size_t ce = chunk * elems;
-  const size_t need = 16 * ce + ce + 4 * (ce / 1024) + 4096;
+  *bytes = 16 * ce + ce + 4 * (ce / 1024) + 4096;
+  return chunk;
+}
+
+// Scratch of `need` bytes: the caller's workspace when given, else the plan's own (grown under
+// the plan's lock, so that two host threads never free and reallocate it at once).
+void* scratch_for(bridct_plan* p, void* workspace, size_t need, int* status) {
+  *status = BRIDCT_OK;
+  if (workspace) return workspace;
+  std::lock_guard<std::mutex> lock(p->tc_mu);
   if (p->tc_bytes < need) {
     if (p->tc_mem) cudaFree(p->tc_mem);
     p->tc_mem = nullptr;
     p->tc_bytes = 0;
     cudaError_t e = cudaMalloc(&p->tc_mem, need);
-    if (e != cudaSuccess) return cuda_fail(e, "FP8 scratch");
+    if (e != cudaSuccess) {
+      *status = cuda_fail(e, "tensor-core scratch");
+      return nullptr;
+    }
     p->tc_bytes = need;
   }
-  float* base = static_cast<float*>(p->tc_mem);
+  return p->tc_mem;
+}
+
+int apply_fp8(bridct_plan* p, int mode, const float* x, float* y, size_t batch, cudaStream_t st, TcDevice* d,
+              void* workspace) {
+  const size_t elems = p->elements;
+  size_t need = 0;
+  const size_t chunk = fp8_chunk(elems, batch, &need);
+  const size_t ce = chunk * elems;
+  int status = BRIDCT_OK;
+  float* base = static_cast<float*>(scratch_for(p, workspace, need, &status));
+  if (!base) return status;
   Fp8Scratch s{base, base + ce, base + 2 * ce, base + 3 * ce, base + 4 * ce, nullptr};
   s.q = reinterpret_cast<uint8_t*>(s.sx + ce / 1024 + 256);
   for (size_t b0 = 0; b0 < batch; b0 += chunk) {
@@ -502,27 +525,28 @@ constexpr size_t kSepChunkBytes = size_t(1024) << 20;
 
 // Separable form: per batch of arrays, pass 1 (rows of W) x -> scratch, pass 2 (rows of H)
 // scratch -> y; the round trip runs the forward pair then the inverse pair on the same batch.
+size_t sep_chunk(size_t elems, size_t batch, size_t* bytes) {
+  size_t chunk = kSepChunkBytes / (elems * sizeof(float));
+  if (chunk < 1) chunk = 1;
+  if (chunk > batch) chunk = batch;
+  *bytes = chunk * elems * sizeof(float);
+  return chunk;
+}
+
 template <int FORM>
-int apply_sep(bridct_plan* p, int mode, const float* x, float* y, size_t batch, cudaStream_t st, TcDevice* d) {
+int apply_sep(bridct_plan* p, int mode, const float* x, float* y, size_t batch, cudaStream_t st, TcDevice* d,
+              void* workspace) {
   if (FORM == tc::BF16X3 && p->h == 64 && p->w == 64) {
     int s = launch_fused64(p, mode == 1, x, y, batch, st, d);
     if (s || mode != 2) return s;
     return launch_fused64(p, true, y, y, batch, st, d);   // each CTA rewrites only tiles it has read
   }
   const size_t elems = (size_t)p->h * p->w;
-  size_t chunk = kSepChunkBytes / (elems * sizeof(float));
-  if (chunk < 1) chunk = 1;
-  if (chunk > batch) chunk = batch;
-  const size_t need = chunk * elems * sizeof(float);
-  if (p->tc_bytes < need) {
-    if (p->tc_mem) cudaFree(p->tc_mem);
-    p->tc_mem = nullptr;
-    p->tc_bytes = 0;
-    cudaError_t e = cudaMalloc(&p->tc_mem, need);
-    if (e != cudaSuccess) return cuda_fail(e, "tensor-core scratch");
-    p->tc_bytes = need;
-  }
-  float* t = static_cast<float*>(p->tc_mem);
+  size_t need = 0;
+  const size_t chunk = sep_chunk(elems, batch, &need);
+  int status = BRIDCT_OK;
+  float* t = static_cast<float*>(scratch_for(p, workspace, need, &status));
+  if (!t) return status;
   const int lh = log2i(p->h), lw = log2i(p->w);
   for (size_t b0 = 0; b0 < batch; b0 += chunk) {
     const size_t nb = batch - b0 < chunk ? batch - b0 : chunk;
@@ -564,7 +588,22 @@ int launch_tc8(const bridct_plan* p, int inverse, const float* x, float* y, size
 
 }  // namespace
 
-int apply_tc_form(bridct_plan* p, int mode, int form, const float* x, float* y, size_t batch, void* stream) {
+size_t tc_workspace_bytes(const bridct_plan* p, int form, size_t batch) {
+  if (!p || batch == 0) return 0;
+  size_t bytes = 0;
+  if (form == BRIDCT_FORM_TC_FP8) {
+    fp8_chunk(p->elements, batch, &bytes);
+    return bytes;
+  }
+  if (form != BRIDCT_FORM_TC_BF16X3 && form != BRIDCT_FORM_TC_TF32X3) return 0;
+  if (p->h == 8 && p->w == 8) return 0;
+  if (form == BRIDCT_FORM_TC_BF16X3 && p->h == 64 && p->w == 64) return 0;
+  sep_chunk(p->elements, batch, &bytes);
+  return bytes;
+}
+
+int apply_tc_form(bridct_plan* p, int mode, int form, const float* x, float* y, size_t batch, void* stream,
+                  void* workspace, size_t) {
   if (!p || !x || !y || mode < 0 || mode > 2 || batch == 0) return BRIDCT_INVALID_ARGUMENT;
   if (form != BRIDCT_FORM_TC_BF16X3 && form != BRIDCT_FORM_TC_TF32X3 && form != BRIDCT_FORM_TC_FP8) {
     set_error("unsupported execution form");
@@ -590,10 +629,10 @@ int apply_tc_form(bridct_plan* p, int mode, int form, const float* x, float* y, 
   TcDevice* d = tc_device(p->device);
   if (!d) return cuda_fail(cudaGetLastError(), "tensor-core setup");
   cudaStream_t st = (cudaStream_t)stream;
-  if (form == BRIDCT_FORM_TC_FP8) return apply_fp8(p, mode, x, y, batch, st, d);
+  if (form == BRIDCT_FORM_TC_FP8) return apply_fp8(p, mode, x, y, batch, st, d, workspace);
   if (!kron)
-    return form == BRIDCT_FORM_TC_BF16X3 ? apply_sep<tc::BF16X3>(p, mode, x, y, batch, st, d)
-                                        : apply_sep<tc::TF32X3>(p, mode, x, y, batch, st, d);
+    return form == BRIDCT_FORM_TC_BF16X3 ? apply_sep<tc::BF16X3>(p, mode, x, y, batch, st, d, workspace)
+                                        : apply_sep<tc::TF32X3>(p, mode, x, y, batch, st, d, workspace);
   int s;
   if (mode == 2) {   // normalized round trip: forward into y, then inverse in place
     s = form == BRIDCT_FORM_TC_BF16X3 ? launch_tc8<tc::BF16X3>(p, 0, x, y, batch, st, d)

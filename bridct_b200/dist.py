@@ -18,13 +18,17 @@ def shard_range(batch: int, rank: int, world: int) -> Tuple[int, int]:
     return first, base + (1 if rank < extra else 0)
 
 
-def max_over_ranks(value: float, device=None) -> float:
-    """Max of a scalar over the default process group (identity without one)."""
+def max_over_ranks(value, device=None):
+    """Max over the default process group of a scalar, or elementwise of a list of scalars
+    (identity without a group)."""
     import torch
     import torch.distributed as dist
 
+    many = isinstance(value, (list, tuple))
+    vals = [float(v) for v in value] if many else [float(value)]
     if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
-        return float(value)
-    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+        return vals if many else vals[0]
+    t = torch.tensor(vals, dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    out = [float(v) for v in t.cpu().tolist()]
+    return out if many else out[0]

@@ -75,12 +75,19 @@ def apply(x: torch.Tensor, mode: int, out: torch.Tensor = None, form: str = "sj"
             raise ValueError("Expected a contiguous, 16-byte aligned output.")
     if batch == 0:
         return out
-    dev = x.device.index if x.device.index is not None else torch.cuda.current_device()
-    plan = _plan(dev, h, w)
-    stream = torch.cuda.current_stream(x.device).cuda_stream
-    st = _lib.lib().bridct_plan_apply_form_device(plan, mode, _FORMS[form], x.data_ptr(), out.data_ptr(),
-                                                  batch, stream)
-    _lib.check(st, "bridct_plan_apply_form_device")
+    L = _lib.lib()
+    fid = _FORMS[form]
+    with torch.cuda.device(x.device):
+        dev = torch.cuda.current_device()
+        plan = _plan(dev, h, w)
+        stream = torch.cuda.current_stream().cuda_stream
+        # A tensor-core form's intermediate comes from torch's caching allocator on this stream, so
+        # that calls from several streams or threads on one cached plan never share scratch.
+        nbytes = L.bridct_plan_form_workspace_bytes(plan, fid, batch)
+        ws = torch.empty(max(1, nbytes), dtype=torch.uint8, device=x.device) if nbytes else None
+        st = L.bridct_plan_apply_form_device_ws(plan, mode, fid, x.data_ptr(), out.data_ptr(), batch,
+                                                ws.data_ptr() if ws is not None else None, nbytes, stream)
+    _lib.check(st, "bridct_plan_apply_form_device_ws")
     return out
 
 

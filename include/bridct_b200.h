@@ -38,9 +38,19 @@ BRIDCT_API const char *bridct_plan_gpu_route(const bridct_plan *plan);
 BRIDCT_API int bridct_plan_apply_batch(bridct_plan *plan, enum bridct_mode mode,
                                        const float *input, float *output, size_t batch);
 
+/* Round trip of `batch` arrays as a FORWARD call followed by an INVERSE call, with the float32
+ * spectrum materialized in the plan's device staging instead of the caller's memory: the result
+ * is bitwise that of the two calls (the NumPy Plan's round trip, python/bridct_numpy.c:119-123
+ * of the reference), but a host batch crosses PCIe once each way.  Host or device pointers;
+ * synchronous.  No reference counterpart. */
+BRIDCT_API int bridct_plan_roundtrip_batch(bridct_plan *plan, const float *input, float *output,
+                                           size_t batch);
+
 /* Device-resident batch: input/output are CUDA device (or managed) pointers to
- * batch*h*w floats, 16-byte aligned.  Asynchronous on `stream` (a cudaStream_t; NULL
- * is the CUDA default stream).  No allocation, no host synchronisation. */
+ * batch*h*w floats, 16-byte aligned, on the plan's device.  Asynchronous on `stream` (a
+ * cudaStream_t of that device; NULL is the CUDA default stream).  The launch runs on the plan's
+ * device whatever device is current, and the caller's current device is left as it was.  No
+ * allocation, no host synchronisation. */
 BRIDCT_API int bridct_plan_apply_device(bridct_plan *plan, enum bridct_mode mode,
                                         const float *input, float *output, size_t batch,
                                         void *stream);
@@ -55,6 +65,21 @@ BRIDCT_API int bridct_plan_apply_device(bridct_plan *plan, enum bridct_mode mode
 BRIDCT_API int bridct_plan_apply_form_device(bridct_plan *plan, enum bridct_mode mode,
                                              enum bridct_form form, const float *input,
                                              float *output, size_t batch, void *stream);
+
+/* Bytes of scratch a form needs for `batch` arrays of the plan's shape when the caller supplies
+ * it (0: the form needs none).  No reference counterpart. */
+BRIDCT_API size_t bridct_plan_form_workspace_bytes(const bridct_plan *plan, enum bridct_form form,
+                                                   size_t batch);
+
+/* As bridct_plan_apply_form_device, with the intermediate in a caller-owned device workspace
+ * (16-byte aligned, at least bridct_plan_form_workspace_bytes bytes; too small ->
+ * BRIDCT_WORKSPACE_TOO_SMALL).  The plan's own scratch is not touched, so calls on one plan may
+ * run on several streams at once, each with its own workspace; a caching allocator that orders
+ * its blocks by stream (PyTorch's) can supply it.  No reference counterpart. */
+BRIDCT_API int bridct_plan_apply_form_device_ws(bridct_plan *plan, enum bridct_mode mode,
+                                                enum bridct_form form, const float *input,
+                                                float *output, size_t batch, void *workspace,
+                                                size_t workspace_bytes, void *stream);
 
 /* Reads and clears the bounded-wait flag of a device: nonzero when a tensor-core kernel's
  * mbarrier wait expired (the kernel then skipped its remaining tiles and returned). */
@@ -112,6 +137,11 @@ BRIDCT_API int bridct_ragged_apply_loop_device(bridct_ragged *batch, const float
                                                float *output, void *stream);
 /* Reads and clears the batch's bounded-wait flag (nonzero: a dependency wait expired). */
 BRIDCT_API int bridct_ragged_timeout_flag(bridct_ragged *batch);
+/* Sets how many times (about 256 ns apart) a row block polls for its array's column strips
+ * before it gives up, skips its rows and raises the batch's timeout flag; the default is
+ * 2^22 (about a second).  0 makes every row block give up at once, which tests use to drive the
+ * timeout path deterministically.  No reference counterpart. */
+BRIDCT_API int bridct_ragged_set_wait_limit(bridct_ragged *batch, unsigned polls);
 
 /* No counterpart in the reference.  The ragged batch for callers that cannot let a library
  * allocate device memory (a framework whose caching allocator owns the whole GPU, a loop that

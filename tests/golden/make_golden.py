@@ -1,7 +1,7 @@
 """Generates tests/golden/*.npz from the reference library (run where the reference tree and
 oracle/_ref exist; the fixtures are committed, this script is not run by the tests).
 
-    python tests/golden/make_golden.py --reference /root/reference
+    python tests/golden/make_golden.py --reference <reference checkout>
 
 Fixtures (each stores inputs `x` and the reference library's outputs `y0`, `y1`, `y2` for
 FORWARD, INVERSE, ROUNDTRIP, computed by oracle/_ref/libbridct_ref.so, i.e. the reference's
@@ -23,6 +23,7 @@ own C code built from its sources):
 from __future__ import annotations
 
 import argparse
+import os
 import hashlib
 import json
 import sys
@@ -108,7 +109,9 @@ def configs() -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", type=Path, default=Path("/root/reference"))
+    env = os.environ.get("BRIDCT_REFERENCE")
+    ap.add_argument("--reference", type=Path, default=Path(env) if env else None, required=env is None,
+                    help="the reference checkout (default: $BRIDCT_REFERENCE)")
     args = ap.parse_args()
     if not O.ref_available():
         raise SystemExit("oracle/_ref/libbridct_ref.so is missing: run `make -C oracle ref` first")

@@ -113,3 +113,34 @@ def test_autotune_picks_a_measured_geometry():
     got = RaggedBatch(items, tuning=res["best"]).apply(x)
     torch.cuda.synchronize()
     close(ref, got, x, items, b)
+
+
+def test_ragged_dependency_wait_expires_and_reports():
+    """The row blocks' bounded wait on their column strips: with a wait limit of zero polls every
+    row block gives up at once, skips its rows and raises the batch's flag; the kernel still
+    returns, the flag reads nonzero once and then clears, tile arrays are unaffected, and with
+    the default limit restored the same batch transforms correctly."""
+    from bridct_b200 import _lib
+
+    L = _lib.lib()
+    items = [(8, 8, 0), (64, 64, 1), (256, 512, 0), (1024, 128, 1), (32, 16, 2), (512, 512, 0)]
+    b = RaggedBatch(items)
+    rng = np.random.default_rng(7)
+    x = torch.from_numpy(rng.uniform(-1, 1, b.span).astype(np.float32)).cuda()
+    y = torch.zeros_like(x)
+    assert L.bridct_ragged_set_wait_limit(b._h, 0) == 0
+    b.apply(x, y)
+    torch.cuda.synchronize()                  # the kernel returned
+    assert b.timed_out()
+    assert not b.timed_out()                  # read and cleared
+    for (h, w, m), xi, yi in zip(items, b.unpack(x), b.unpack(y)):
+        if h * w <= 16384:                    # whole-array units never wait
+            xi, yi = xi.cpu().numpy(), yi.cpu().numpy()
+            assert O.rel_max_error(yi, O.fp64_apply(xi, m), xi, output_scaled=True) <= TOL, (h, w, m)
+    assert L.bridct_ragged_set_wait_limit(b._h, 1 << 22) == 0
+    y = b.apply(x)
+    torch.cuda.synchronize()
+    assert not b.timed_out()
+    for (h, w, m), xi, yi in zip(items, b.unpack(x), b.unpack(y)):
+        xi, yi = xi.cpu().numpy(), yi.cpu().numpy()
+        assert O.rel_max_error(yi, O.fp64_apply(xi, m), xi, output_scaled=True) <= TOL, (h, w, m)

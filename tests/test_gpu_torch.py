@@ -49,3 +49,35 @@ def test_errors():
         torch_api.dct2(torch.zeros(8, 8, device="cuda", dtype=torch.float64))
     with pytest.raises(ValueError):
         torch_api.dct2(torch.zeros(8, 12, device="cuda"))
+
+
+@pytest.mark.parametrize("form", ["tc_bf16x3", "tc_tf32x3"])
+def test_tensor_core_form_on_two_streams_of_one_cached_plan(form):
+    """Two side streams run the same shape's tensor-core form at once through the one cached
+    plan: each call's intermediate comes from torch's allocator on its own stream, so the results
+    equal the same calls made one at a time."""
+    xa = torch.randn(512, 128, 256, device="cuda")
+    xb = torch.randn(512, 128, 256, device="cuda")
+    ref_a = torch_api.apply(xa, 0, form=form)
+    ref_b = torch_api.apply(xb, 0, form=form)
+    torch.cuda.synchronize()
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    outs = []
+    for _ in range(3):
+        with torch.cuda.stream(s1):
+            ya = torch_api.apply(xa, 0, form=form)
+        with torch.cuda.stream(s2):
+            yb = torch_api.apply(xb, 0, form=form)
+        outs.append((ya, yb))
+    torch.cuda.synchronize()
+    for ya, yb in outs:
+        assert torch.equal(ya, ref_a) and torch.equal(yb, ref_b)
+
+
+def test_calls_leave_the_current_device_unchanged():
+    dev = torch.cuda.current_device()
+    x = torch.randn(4, 256, 256, device=f"cuda:{dev}")
+    torch_api.dct2(x)
+    torch_api.apply(x, 0, form="tc_bf16x3")
+    torch.cuda.synchronize()
+    assert torch.cuda.current_device() == dev

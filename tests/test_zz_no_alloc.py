@@ -5,8 +5,10 @@ caching allocator owns the whole GPU, a loop that cannot afford cudaMalloc's imp
 synchronisation, or a process with a fixed device footprint.  The entry point keeps its work
 queue, counters and tables in one static device array.  These tests call it through the C-ABI
 twice in a row, with different batches, and compare each result with the allocating entry
-point (bridct_ragged_create + bridct_ragged_apply_device) within the parity bound.  The file is
-collected last, and passes both alone in a fresh process and after the other tests.
+point (bridct_ragged_create + bridct_ragged_apply_device) within the parity bound, and a sample
+of each call's arrays (the 1024x1024 two-pass array, four-step arrays with 128/256/512 axes and
+small tiles) directly with the float64 transform.  The file is collected last, and passes both
+alone in a fresh process and after the other tests.
 """
 import numpy as np
 import pytest
@@ -24,7 +26,13 @@ def _items(seed, n):
     rng = np.random.default_rng(seed)
     out = [(int(rng.choice(SIZES)), int(rng.choice(SIZES)), int(rng.integers(0, 3))) for _ in range(n)]
     out += [(1024, 1024, 0), (8, 8, 1), (128, 1024, 2)]       # two-pass, tile and rect arrays
+    out += [(128, 256, 1), (256, 512, 0), (512, 128, 2)]      # four-step lines of every width
     return out
+
+
+def _fp64_sample(items):
+    """Indices checked against float64: the appended arrays plus every 15th random one."""
+    return sorted(set(range(len(items) - 6, len(items))) | set(range(0, len(items) - 6, 15)))
 
 
 def _c_items(batch):
@@ -49,6 +57,11 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls():
             xi, yi, ri = xi.cpu().numpy(), yi.cpu().numpy(), ri.cpu().numpy()
             assert np.isfinite(yi).all(), (h, w, m)
             assert O.rel_max_error(yi, ri, xi, output_scaled=True) <= TOL, (h, w, m)
+        xs, ys = ref_batch.unpack(x), ref_batch.unpack(y)
+        for i in _fp64_sample(items):
+            h, w, m = items[i]
+            xi, yi = xs[i].cpu().numpy(), ys[i].cpu().numpy()
+            assert O.rel_max_error(yi, O.fp64_apply(xi, m), xi, output_scaled=True) <= TOL, (h, w, m)
 
 
 def test_noalloc_rejects_batches_beyond_its_maximum():
