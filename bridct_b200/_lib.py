@@ -57,6 +57,8 @@ def lib() -> C.CDLL:
     _sig(L, "bridct_plan_roundtrip_batch", C.c_int, [vp, vp, vp, C.c_size_t])
     _sig(L, "bridct_plan_apply_device", C.c_int, [vp, C.c_int, vp, vp, C.c_size_t, vp])
     _sig(L, "bridct_plan_apply_form_device", C.c_int, [vp, C.c_int, C.c_int, vp, vp, C.c_size_t, vp])
+    _sig(L, "bridct_plan_apply_strided_device", C.c_int, [vp, C.c_int, vp, C.c_size_t, C.c_size_t, vp,
+                                                          C.c_size_t, C.c_size_t, C.c_size_t, vp])
     _sig(L, "bridct_plan_synchronize", C.c_int, [vp])
     for name, res, args in EXTRA_SIGNATURES:
         if hasattr(L, name):

@@ -193,10 +193,14 @@ const void* device_address(const void* p, bool* pinned) {
 
 int launch_plain_form(const bridct_plan* p, int mode, const float* x, float* y, long long batch,
                       cudaStream_t st) {
-  DeviceCtx* d = p->dev;
-  LineTables tab{d->tables(p->h), d->tables(p->w)};
-  PlainLauncher fn = d->plain[lg2(p->h)][lg2(p->w)][mode];
-  cudaError_t e = fn(x, y, batch, st, tab, d->launch);
+  return launch_plain_layout(p->dev, p->h, p->w, mode, x, y, batch, nullptr, nullptr, st);
+}
+
+int launch_plain_layout(DeviceCtx* d, int h, int w, int mode, const float* x, float* y, long long batch,
+                        const BatchLayout* lx, const BatchLayout* ly, cudaStream_t st) {
+  LineTables tab{d->tables(h), d->tables(w)};
+  PlainLauncher fn = d->plain[lg2(h)][lg2(w)][mode];
+  cudaError_t e = fn(x, y, batch, st, tab, d->launch, lx, ly);
   if (e != cudaSuccess) return cuda_fail(e, "plain kernel launch");
   return BRIDCT_OK;
 }
@@ -363,6 +367,48 @@ BRIDCT_API int bridct_plan_apply_device(bridct_plan* plan, enum bridct_mode mode
   if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(plan device)");
   // NULL is the CUDA default stream, as everywhere in CUDA (torch's default stream too).
   return launch_plain_form(plan, mode, input, output, (long long)batch, (cudaStream_t)stream);
+}
+
+// Floats from the first element of a strided batch to one past its last.
+static size_t strided_extent(size_t h, size_t w, size_t ld, size_t bs, size_t batch) {
+  return (batch - 1) * bs + (h - 1) * ld + w;
+}
+
+// A strided layout writes every element once: arrays apart (bs covers a whole array), or arrays
+// side by side within every row band (bs covers a row, ld covers the batch's row).
+static bool strided_disjoint(size_t h, size_t w, size_t ld, size_t bs, size_t batch) {
+  if (ld < w) return false;
+  if (batch == 1 || bs >= (h - 1) * ld + w) return true;
+  return bs >= w && ld >= (batch - 1) * bs + w;
+}
+
+BRIDCT_API int bridct_plan_apply_strided_device(bridct_plan* plan, enum bridct_mode mode, const float* input,
+                                                size_t input_row_pitch, size_t input_array_stride, float* output,
+                                                size_t output_row_pitch, size_t output_array_stride, size_t batch,
+                                                void* stream) {
+  if (!plan || !input || !output || (unsigned)mode > BRIDCT_ROUNDTRIP || batch == 0) return BRIDCT_INVALID_ARGUMENT;
+  const size_t h = plan->h, w = plan->w;
+  if (!strided_disjoint(h, w, input_row_pitch, input_array_stride, batch) ||
+      !strided_disjoint(h, w, output_row_pitch, output_array_stride, batch)) {
+    set_error("bridct_plan_apply_strided_device: row pitch below the width, or arrays that overlap");
+    return BRIDCT_INVALID_ARGUMENT;
+  }
+  if ((input_row_pitch | output_row_pitch | (batch > 1 ? input_array_stride | output_array_stride : 0)) % 4 ||
+      ((uintptr_t)input | (uintptr_t)output) % 16) {
+    set_error("bridct_plan_apply_strided_device: pitches and strides must be multiples of 4 floats and the "
+              "pointers 16-byte aligned");
+    return BRIDCT_BAD_ALIGNMENT;
+  }
+  const size_t xe = strided_extent(h, w, input_row_pitch, input_array_stride, batch);
+  const size_t ye = strided_extent(h, w, output_row_pitch, output_array_stride, batch);
+  const uintptr_t a = (uintptr_t)input, b = (uintptr_t)output;
+  if (a <= b ? b - a < xe * sizeof(float) : a - b < ye * sizeof(float)) return BRIDCT_OVERLAPPING_BUFFERS;
+  DeviceGuard guard(plan->device);
+  if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(plan device)");
+  const BatchLayout lx{nullptr, (long long)input_array_stride, (long long)input_row_pitch};
+  const BatchLayout ly{nullptr, (long long)output_array_stride, (long long)output_row_pitch};
+  return launch_plain_layout(plan->dev, plan->h, plan->w, mode, input, output, (long long)batch, &lx, &ly,
+                             (cudaStream_t)stream);
 }
 
 BRIDCT_API int bridct_plan_synchronize(bridct_plan* plan) {

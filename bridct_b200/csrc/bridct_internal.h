@@ -93,6 +93,9 @@ namespace bridct {
 constexpr int kModeSpectrumRT = 3;
 int launch_plain_form(const bridct_plan* p, int mode, const float* x, float* y, long long batch,
                       cudaStream_t st);
+// Plain form over `batch` h x w arrays on device d in general layouts (lx, ly NULL: contiguous).
+int launch_plain_layout(DeviceCtx* d, int h, int w, int mode, const float* x, float* y, long long batch,
+                        const BatchLayout* lx, const BatchLayout* ly, cudaStream_t st);
 int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, size_t batch,
                         const float* dx, float* dy, bool pin_in, bool pin_out);
 bridct_plan* thread_square_plan(int n);

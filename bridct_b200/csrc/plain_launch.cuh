@@ -10,8 +10,9 @@ struct LaunchCtx {
   int sm_count;
 };
 
+// lx, ly: general layouts of x and y (both NULL: a contiguous batch).
 using PlainLauncher = cudaError_t (*)(const float*, float*, long long, cudaStream_t,
-                                      LineTables, const LaunchCtx&);
+                                      LineTables, const LaunchCtx&, const BatchLayout*, const BatchLayout*);
 
 int kernel_setup(const void* kernel, int smem, int threads);   // bridct_api.cu
 
@@ -32,12 +33,16 @@ static cudaError_t launch_tiles(Kernel k, int smem, int bps, TileArgs a, const L
   return cudaGetLastError();
 }
 
-template <int H, int W, int MODE>
-cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t st,
-                         LineTables tab, const LaunchCtx& ctx) {
+// GEN: the batch has general layouts (strided arrays or an offset table, BatchLayout); the same
+// geometry choices run the GEN instantiations of the kernels, except that 8x8 arrays take the
+// generic tile kernel instead of the dedicated one-thread-per-array kernels.
+template <int H, int W, int MODE, bool GEN>
+cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStream_t st,
+                              LineTables tab, const LaunchCtx& ctx, const BatchLayout& lx,
+                              const BatchLayout& ly) {
   using Gm = Geometry<H, W>;
   if (batch <= 0) return cudaSuccess;
-  if constexpr (H == 8 && W == 8) {
+  if constexpr (H == 8 && W == 8 && !GEN) {
     // Measured on B200 (GB/s, device-resident, back-to-back launches): the double-buffered kernel
     // wins forward/inverse batches up to a few hundred thousand arrays (262,144: 5131 vs 4937)
     // and round trips from about 200,000 (524,288: 5655 vs 5130); the single-buffer kernel
@@ -78,18 +83,18 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
     // round trips +3..30% together with their register lines).  Forward / inverse tiles that mix
     // 128-point register lines with many short lines measured 5..13% slower that way.
     constexpr int T = (H == 128 && W == 128) || (MODE == LM_RT && (H == 128 || W == 128)) ? 128 : kThreads;
-    auto k = k_full<H, W, TR, true, true, MODE, T>;
+    auto k = k_full<H, W, TR, true, true, MODE, T, GEN>;
     const int bps = kernel_blocks_per_sm(k, smem, T);
-    TileArgs a{x, y, (batch * H + TR - 1) / TR, batch * H, tab};
+    TileArgs a{x, y, (batch * H + TR - 1) / TR, batch * H, tab, lx, ly};
     return launch_tiles(k, smem, bps, a, ctx, st, T);
   } else if constexpr (H * W == 32768 && (MODE == LM_INV || H == 1024 || H == 64 || (H == 32 && MODE == LM_FWD))) {
     // Whole 32768-float arrays as tiles (one CTA per SM, both passes in shared memory) instead of
     // the two passes, where that measured faster: every inverse (+5..21%), forward of 1024 x 32,
     // 32 x 1024 and 64 x 512 (+2..14%), round trips of 1024 x 32 and 64 x 512 (+2..6%); round
     // trips of 128 x 256 and 256 x 128 measured 30% slower.
-    auto k = k_full<H, W, H, true, true, MODE>;
+    auto k = k_full<H, W, H, true, true, MODE, kThreads, GEN>;
     const int bps = kernel_blocks_per_sm(k, Gm::kSmemWhole);
-    TileArgs a{x, y, batch, batch * H, tab};
+    TileArgs a{x, y, batch, batch * H, tab, lx, ly};
     return launch_tiles(k, Gm::kSmemWhole, bps, a, ctx, st);
   } else {
     // Round trips of 128-point register lines run 128-thread CTAs without register prefetch:
@@ -97,8 +102,8 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
     // CTA with prefetch; forward and inverse measured 5..9% slower that way and keep 256 threads.
     constexpr int TC_T = H == 128 && MODE == LM_RT ? 128 : kThreads;
     constexpr int TR_T = W == 128 && MODE == LM_RT ? 128 : kThreads;
-    auto kc = k_colstrip<H, W, Gm::kTC, MODE, TC_T>;
-    auto kr = k_full<H, W, Gm::kRB, false, true, MODE, TR_T>;
+    auto kc = k_colstrip<H, W, Gm::kTC, MODE, TC_T, GEN>;
+    auto kr = k_full<H, W, Gm::kRB, false, true, MODE, TR_T, GEN>;
     const int bpc = kernel_blocks_per_sm(kc, Gm::kSmemStrip, TC_T);
     const int bpr = kernel_blocks_per_sm(kr, Gm::kSmemRows, TR_T);
     // One column-strip launch and one row-block launch over the whole batch.  Cutting the batch
@@ -109,25 +114,32 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
     const long long nb = batch;
     cudaError_t e;
     if (nb * (W / Gm::kTC) < 2LL * ctx.sm_count) {   // few arrays: smaller strips and row blocks
-      auto kcs = k_colstrip<H, W, Gm::kTCs, MODE, TC_T>;
-      TileArgs ac{x, y, nb * (W / Gm::kTCs), nb * H, tab};
+      auto kcs = k_colstrip<H, W, Gm::kTCs, MODE, TC_T, GEN>;
+      TileArgs ac{x, y, nb * (W / Gm::kTCs), nb * H, tab, lx, ly};
       e = launch_tiles(kcs, Gm::kSmemStripS, kernel_blocks_per_sm(kcs, Gm::kSmemStripS, TC_T), ac, ctx, st, TC_T);
     } else {
-      TileArgs ac{x, y, nb * (W / Gm::kTC), nb * H, tab};
+      TileArgs ac{x, y, nb * (W / Gm::kTC), nb * H, tab, lx, ly};
       e = launch_tiles(kc, Gm::kSmemStrip, bpc, ac, ctx, st, TC_T);
     }
     if (e != cudaSuccess) return e;
     if (nb * H / Gm::kRB < 2LL * ctx.sm_count) {
-      auto krs = k_full<H, W, Gm::kRBs, false, true, MODE, TR_T>;
-      TileArgs ar{y, y, nb * H / Gm::kRBs, nb * H, tab};
+      auto krs = k_full<H, W, Gm::kRBs, false, true, MODE, TR_T, GEN>;
+      TileArgs ar{y, y, nb * H / Gm::kRBs, nb * H, tab, ly, ly};
       e = launch_tiles(krs, Gm::kSmemRowsS, kernel_blocks_per_sm(krs, Gm::kSmemRowsS, TR_T), ar, ctx, st, TR_T);
     } else {
-      TileArgs ar{y, y, nb * H / Gm::kRB, nb * H, tab};
+      TileArgs ar{y, y, nb * H / Gm::kRB, nb * H, tab, ly, ly};
       e = launch_tiles(kr, Gm::kSmemRows, bpr, ar, ctx, st, TR_T);
     }
     if (e != cudaSuccess) return e;
     return cudaSuccess;
   }
+}
+
+template <int H, int W, int MODE>
+cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t st, LineTables tab,
+                         const LaunchCtx& ctx, const BatchLayout* lx, const BatchLayout* ly) {
+  if (lx && ly) return launch_plain_impl<H, W, MODE, true>(x, y, batch, st, tab, ctx, *lx, *ly);
+  return launch_plain_impl<H, W, MODE, false>(x, y, batch, st, tab, ctx, BatchLayout{}, BatchLayout{});
 }
 
 // Per-H instantiation units (plain_inst.cu compiled once per H) export this table row.

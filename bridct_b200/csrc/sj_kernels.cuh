@@ -37,13 +37,33 @@ struct LineTables {
   FourStepTables row;   // for line length w (used when w >= 128)
 };
 
+// Where the arrays of a launch live in a general layout (kernels instantiated with GEN): array b
+// starts at offs[b] when an offset table is given (the shape classes of a ragged batch), else at
+// b * bs (a strided batch), and its rows are ld floats apart.  Array starts and ld are multiples of
+// 4 floats, so every row is 16-byte aligned.  Contiguous batches (array b at b*h*w, rows w apart)
+// use the kernels' fixed addressing instead.
+struct BatchLayout {
+  const long long* offs = nullptr;
+  long long bs = 0;
+  long long ld = 0;
+};
+
 struct TileArgs {
   const float* x;
   float* y;
   long long ntiles;
   long long rows_total;   // rows of the (batch*h) x w matrix covered by this launch
   LineTables tab;
+  BatchLayout lx, ly;     // layouts of x and y (GEN kernels only)
 };
+
+// Offset (floats) of row g of the (batch*H) x W row matrix in a general layout.
+template <int H>
+__device__ __forceinline__ long long layout_row(const BatchLayout& l, long long g) {
+  const long long b = g / H;
+  const int r = (int)(g % H);
+  return (l.offs ? __ldg(l.offs + b) : b * l.bs) + (long long)r * l.ld;
+}
 
 template <int N> struct ExchangeFloats { static constexpr int value = 0; };
 template <> struct ExchangeFloats<128> { static constexpr int value = FourStepSizes<4>::FLOATS; };
@@ -166,6 +186,19 @@ struct TileRegs {
       }
     }
   }
+  // As load, with row r of the tile at rp(r).
+  template <typename RowPtr>
+  __device__ __forceinline__ void load_rows(const RowPtr& rp, int valid_rows) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      const int i = threadIdx.x + k * THREADS;
+      if (ROWS * Q % THREADS == 0 || i < ROWS * Q) {
+        const int r = i / Q, c = (i % Q) * 4;
+        v[k] = r < valid_rows ? __ldg(reinterpret_cast<const float4*>(rp(r) + c))
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+  }
   __device__ __forceinline__ void put(float* tile) const {
 #pragma unroll
     for (int k = 0; k < N; ++k) {
@@ -185,6 +218,54 @@ struct TileRegs {
     }
   }
 };
+
+// tile_load for tiles whose rows lie anywhere (row r at rp(r), 16-byte aligned).
+template <int P, typename RowPtr>
+__device__ __forceinline__ void tile_load_rows(const RowPtr& rp, int rows, int cols, float* tile, int valid_rows) {
+  const int q = cols / 4;
+  for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
+    const int r = i / q, c = (i % q) * 4;
+    float* d = tile + r * P + c;
+    if constexpr (P % 2 == 0) {
+      if (r < valid_rows) {
+        const float* src = rp(r) + c;
+        if constexpr (P % 4 == 0) {
+          cp_async16(d, src);
+        } else {
+          cp_async8(d, src);
+          cp_async8(d + 2, src + 2);
+        }
+      } else {
+        d[0] = 0.f; d[1] = 0.f; d[2] = 0.f; d[3] = 0.f;
+      }
+    } else {
+      const float4 v = r < valid_rows ? __ldg(reinterpret_cast<const float4*>(rp(r) + c))
+                                      : make_float4(0.f, 0.f, 0.f, 0.f);
+      d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+    }
+  }
+  if constexpr (P % 2 == 0) cp_async_wait_all();
+}
+
+// tile_store for tiles whose rows lie anywhere; rows from valid_rows on are not stored.
+template <int P, typename RowPtr>
+__device__ __forceinline__ void tile_store_rows(const RowPtr& rp, int rows, int cols, const float* tile) {
+  const int q = cols / 4;
+  for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
+    const int r = i / q, c = (i % q) * 4;
+    const float* sp = tile + r * P + c;
+    float4 v;
+    if constexpr (P % 4 == 0) {
+      v = *reinterpret_cast<const float4*>(sp);
+    } else if constexpr (P % 2 == 0) {
+      const float2 lo = reinterpret_cast<const float2*>(sp)[0], hi = reinterpret_cast<const float2*>(sp)[1];
+      v = make_float4(lo.x, lo.y, hi.x, hi.y);
+    } else {
+      v = make_float4(sp[0], sp[1], sp[2], sp[3]);
+    }
+    *reinterpret_cast<float4*>(rp(r) + c) = v;
+  }
+}
 
 template <int P>
 __device__ __forceinline__ void tile_store(float* g, long long gp, int rows, int cols, const float* tile) {
@@ -227,7 +308,7 @@ __device__ __forceinline__ void run_lines(float* tile, int nlines, int es, const
 
 // Full-width tiles: TR consecutive rows (of width W) of the batch viewed as a (B*H) x W
 // matrix.  With DO_COL the tile holds TR/H whole arrays.
-template <int H, int W, int TR, bool DO_COL, bool DO_ROW, int MODE, int THREADS = kThreads>
+template <int H, int W, int TR, bool DO_COL, bool DO_ROW, int MODE, int THREADS = kThreads, bool GEN = false>
 __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
   constexpr int P = DO_COL ? pitch_of(H, W, true) : rowblock_pitch(W);
   constexpr int XB = (THREADS / 32) * cmax(DO_COL ? ExchangeFloats<H>::value : 0, DO_ROW ? ExchangeFloats<W>::value : 0);
@@ -252,16 +333,30 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
   constexpr bool kPrefetch = THREADS == kThreads && TR * W <= 16384 &&
                              (DO_COL ? DO_ROW && (H >= 128 || W >= 128) && !(W >= 256 && TR * W >= 16384)
                                      : (DO_ROW && W == 128));
+  // General layouts (GEN): row r of tile t is row t * TR + r of the batch's row matrix.
+  auto xrow = [&](long long t) {
+    return [&a, t](int r) { return a.x + layout_row<H>(a.lx, t * TR + r); };
+  };
+  auto yrow = [&](long long t) {
+    return [&a, t](int r) { return a.y + layout_row<H>(a.ly, t * TR + r); };
+  };
   TileRegs<P, kPrefetch ? TR : 4, kPrefetch ? W : 4, THREADS> next;
-  if (kPrefetch && blockIdx.x < a.ntiles) next.load(a.x + blockIdx.x * (long long)TR * W, W, rows_of(blockIdx.x));
+  if (kPrefetch && blockIdx.x < a.ntiles) {
+    if constexpr (GEN) next.load_rows(xrow(blockIdx.x), rows_of(blockIdx.x));
+    else next.load(a.x + blockIdx.x * (long long)TR * W, W, rows_of(blockIdx.x));
+  }
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const int rows = rows_of(t);
     if constexpr (kPrefetch) {
       next.put(tile);
       __syncthreads();
-      if (t + gridDim.x < a.ntiles) next.load(a.x + (t + gridDim.x) * (long long)TR * W, W, rows_of(t + gridDim.x));
+      if (t + gridDim.x < a.ntiles) {
+        if constexpr (GEN) next.load_rows(xrow(t + gridDim.x), rows_of(t + gridDim.x));
+        else next.load(a.x + (t + gridDim.x) * (long long)TR * W, W, rows_of(t + gridDim.x));
+      }
     } else {
-      tile_load<P>(a.x + t * (long long)TR * W, W, TR, W, tile, rows);
+      if constexpr (GEN) tile_load_rows<P>(xrow(t), TR, W, tile, rows);
+      else tile_load<P>(a.x + t * (long long)TR * W, W, TR, W, tile, rows);
       __syncthreads();
     }
     if constexpr (DO_COL) {
@@ -274,13 +369,15 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
       run_lines<W, MODE, reg_line_max(W, H, MODE, !DO_COL)>(tile, TR, 1, [](int l) { return l * P; }, xbuf, trow);
       __syncthreads();
     }
-    tile_store<P>(a.y + t * (long long)TR * W, W, rows, W, tile);
+    if constexpr (GEN) tile_store_rows<P>(yrow(t), rows, W, tile);
+    else tile_store<P>(a.y + t * (long long)TR * W, W, rows, W, tile);
     __syncthreads();
   }
 }
 
-// Column strips: H rows x TC columns of one array (row pitch W in global memory).
-template <int H, int W, int TC, int MODE, int THREADS = kThreads>
+// Column strips: H rows x TC columns of one array (row pitch W in global memory; ld of the
+// layouts with GEN).
+template <int H, int W, int TC, int MODE, int THREADS = kThreads, bool GEN = false>
 __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
   constexpr int P = strip_pitch(H, TC);
   constexpr int STRIPS = W / TC;
@@ -291,23 +388,26 @@ __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
   // Strips of 128- and 256-point columns prefetch the next strip into registers during the
   // transform; longer columns keep their occupancy.
   constexpr bool kPrefetch = THREADS == kThreads && (H == 128 || H == 256);
-  auto src = [&](long long t) { return a.x + (t / STRIPS) * (long long)H * W + (t % STRIPS) * TC; };
+  const long long xp = GEN ? a.lx.ld : W, yp = GEN ? a.ly.ld : W;
+  auto xarr = [&](long long arr) { return GEN ? a.x + layout_row<H>(a.lx, arr * H) : a.x + arr * (long long)H * W; };
+  auto yarr = [&](long long arr) { return GEN ? a.y + layout_row<H>(a.ly, arr * H) : a.y + arr * (long long)H * W; };
+  auto src = [&](long long t) { return xarr(t / STRIPS) + (t % STRIPS) * TC; };
   TileRegs<P, kPrefetch ? H : 4, kPrefetch ? TC : 4, THREADS> next;
-  if (kPrefetch && blockIdx.x < a.ntiles) next.load(src(blockIdx.x), W, H);
+  if (kPrefetch && blockIdx.x < a.ntiles) next.load(src(blockIdx.x), xp, H);
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const long long arr = t / STRIPS;
     const int s = (int)(t % STRIPS);
     if constexpr (kPrefetch) {
       next.put(tile);
       __syncthreads();
-      if (t + gridDim.x < a.ntiles) next.load(src(t + gridDim.x), W, H);
+      if (t + gridDim.x < a.ntiles) next.load(src(t + gridDim.x), xp, H);
     } else {
-      tile_load<P>(a.x + arr * (long long)H * W + s * TC, W, H, TC, tile, H);
+      tile_load<P>(xarr(arr) + s * TC, xp, H, TC, tile, H);
       __syncthreads();
     }
     run_lines<H, MODE, reg_line_max(H, W, MODE, true)>(tile, TC, P, [](int l) { return l; }, xbuf, tcol);
     __syncthreads();
-    tile_store<P>(a.y + arr * (long long)H * W + s * TC, W, H, TC, tile);
+    tile_store<P>(yarr(arr) + s * TC, yp, H, TC, tile);
     __syncthreads();
   }
 }

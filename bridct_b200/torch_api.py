@@ -58,11 +58,42 @@ def _check(x: torch.Tensor) -> Tuple[int, int, int]:
     return h, w, batch
 
 
+def _strides(t: torch.Tensor):
+    """(row pitch, array stride) in floats when the kernels can address t where it lies: unit
+    column stride, leading dimensions that flatten to one array stride, multiples of 4 floats and a
+    16-byte aligned start; else None."""
+    if t.stride(-1) != 1 or t.data_ptr() % 16:
+        return None
+    ld = t.stride(-2) if t.shape[-2] > 1 else t.shape[-1]
+    lead = [(n, s) for n, s in zip(t.shape[:-2], t.stride()[:-2]) if n != 1]
+    bs = lead[-1][1] if lead else t.shape[-2] * ld
+    for i in range(len(lead) - 1):
+        if lead[i][1] != lead[i + 1][1] * lead[i + 1][0]:
+            return None
+    if ld % 4 or bs % 4 or ld < t.shape[-1]:
+        return None
+    return ld, bs
+
+
 def apply(x: torch.Tensor, mode: int, out: torch.Tensor = None, form: str = "sj") -> torch.Tensor:
-    """Transforms the last two axes of a CUDA float32 tensor (no autograd)."""
+    """Transforms the last two axes of a CUDA float32 tensor (no autograd).
+
+    The plain form reads strided views where they lie (sub-images, slices, permuted batch axes
+    whose last axis has unit stride; row pitch and array stride multiples of 4 floats) and writes
+    `out` likewise; other layouts, and the tensor-core forms, get a contiguous copy first."""
     h, w, batch = _check(x)
     if form not in _FORMS:
         raise ValueError(f"unknown form {form!r}; expected one of {sorted(_FORMS)}")
+    if form == "sj" and batch > 0 and not x.is_contiguous():
+        sx = _strides(x)
+        if sx is not None:
+            if out is None:
+                out = torch.empty(x.shape, dtype=torch.float32, device=x.device)
+            elif out.shape != x.shape or out.dtype != torch.float32 or out.device != x.device:
+                raise ValueError("Input and output shapes must match exactly.")
+            so = _strides(out)
+            if so is not None:
+                return _apply_strided(x, sx, out, so, mode, h, w, batch)
     x = x.contiguous()
     if x.data_ptr() % 16:
         x = x.clone()
@@ -88,6 +119,16 @@ def apply(x: torch.Tensor, mode: int, out: torch.Tensor = None, form: str = "sj"
         st = L.bridct_plan_apply_form_device_ws(plan, mode, fid, x.data_ptr(), out.data_ptr(), batch,
                                                 ws.data_ptr() if ws is not None else None, nbytes, stream)
     _lib.check(st, "bridct_plan_apply_form_device_ws")
+    return out
+
+
+def _apply_strided(x, sx, out, so, mode, h, w, batch):
+    L = _lib.lib()
+    with torch.cuda.device(x.device):
+        plan = _plan(torch.cuda.current_device(), h, w)
+        st = L.bridct_plan_apply_strided_device(plan, mode, x.data_ptr(), sx[0], sx[1], out.data_ptr(), so[0], so[1],
+                                                batch, torch.cuda.current_stream().cuda_stream)
+    _lib.check(st, "bridct_plan_apply_strided_device")
     return out
 
 

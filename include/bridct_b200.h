@@ -55,6 +55,20 @@ BRIDCT_API int bridct_plan_apply_device(bridct_plan *plan, enum bridct_mode mode
                                         const float *input, float *output, size_t batch,
                                         void *stream);
 
+/* Device-resident strided batch (plain form): element (r, c) of array b is read at
+ * input[b * input_array_stride + r * input_row_pitch + c] and written at the same place of output
+ * with the output's pitch and stride (all in floats).  Sub-images, tensor slices and arrays side by
+ * side in a wider image transform where they lie, with no copy.  Pitches and strides must be
+ * multiples of 4 floats and the pointers 16-byte aligned (else BRIDCT_BAD_ALIGNMENT); a pitch below
+ * the width or arrays that overlap -> BRIDCT_INVALID_ARGUMENT; input and output extents that
+ * overlap -> BRIDCT_OVERLAPPING_BUFFERS.  Asynchronous on `stream`, on the plan's device, no
+ * allocation.  The reference accepts contiguous arrays only (docs/API.md:17). */
+BRIDCT_API int bridct_plan_apply_strided_device(bridct_plan *plan, enum bridct_mode mode,
+                                                const float *input, size_t input_row_pitch,
+                                                size_t input_array_stride, float *output,
+                                                size_t output_row_pitch, size_t output_array_stride,
+                                                size_t batch, void *stream);
+
 /* As bridct_plan_apply_device, with an explicit execution form (precision forms run
  * on the tensor cores; see enum bridct_form for the shapes each form supports).  The
  * tensor-core forms on axes of 64..256 and the FP8 form keep their intermediate in scratch
