@@ -12,6 +12,7 @@ FORWARD, INVERSE, ROUNDTRIP = 0, 1, 2
 OK, INVALID_ARGUMENT, WORKSPACE_TOO_SMALL, BAD_ALIGNMENT, OVERLAPPING_BUFFERS = 0, -1, -2, -3, -4
 DEVICE_ERROR, TIMEOUT = -5, -6
 FORM_SJ, FORM_TC_BF16X3, FORM_TC_TF32X3, FORM_TC_FP8 = 0, 1, 2, 3
+RAGGED_QUEUE, RAGGED_CLASS_LAUNCH, RAGGED_CLASS_LAUNCH_SMALL = 0, 1, 2
 VERSION = "0.2.0-dev.7"
 
 _FP = C.POINTER(C.c_float)
@@ -78,6 +79,12 @@ EXTRA_SIGNATURES = [
     ("bridct_ragged_apply_loop_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("bridct_ragged_timeout_flag", C.c_int, [C.c_void_p]),
     ("bridct_ragged_set_wait_limit", C.c_int, [C.c_void_p, C.c_uint]),
+    ("bridct_ragged_class_count", C.c_size_t, [C.c_void_p]),
+    ("bridct_ragged_class_info", C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                           C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_int)]),
+    ("bridct_ragged_set_schedule", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_size_t, C.c_int]),
+    ("bridct_ragged_apply_class_device", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_void_p, C.c_void_p,
+                                                   C.c_void_p]),
     ("bridct_device_timeout_flag", C.c_int, [C.c_int]),
     ("bridct_ragged_apply_noalloc", C.c_int, [C.POINTER(RaggedItem), C.c_size_t, C.c_void_p, C.c_void_p,
                                               C.c_void_p]),

@@ -93,3 +93,79 @@ def tune(items, x, candidates: Optional[Dict[str, Sequence[int]]] = None, sweeps
         if not improved:
             break
     return {"best": best, "best_ms": best_ms, "default_ms": base_ms, "table": table}
+
+
+def _time_graph(fn, x, steps: int) -> float:
+    """Milliseconds per call of fn(stream) from a CUDA graph of `steps` calls (after a warm replay)."""
+    import torch
+
+    stream = torch.cuda.Stream(device=x.device)
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            fn(stream.cuda_stream)
+    stream.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        for _ in range(steps):
+            fn(stream.cuda_stream)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        g.replay()
+        start.record(stream)
+        g.replay()
+        end.record(stream)
+    end.synchronize()
+    del g
+    return start.elapsed_time(end) / steps
+
+
+def tune_classes(items, x, tuning: Optional[Dict[str, int]] = None, steps: int = 8,
+                 streams: Sequence[int] = (1, 2, 4, 8)) -> Dict[str, object]:
+    """Per-shape-class schedules of a ragged batch.
+
+    Every shape class (height, width, mode) is timed alone in each schedule: in the persistent
+    queue (a batch of that class's arrays only, at their own offsets), as its own fixed-shape
+    launch, and for two-pass shapes with the few-array geometry; the fastest wins.  The chosen
+    schedule is then timed on the whole batch for each side-stream count, next to the all-queue
+    and all-launch schedules, and the fastest whole-batch schedule is returned (its output checked
+    against the all-queue result).  Returns {"schedule", "ms", "queue_ms", "launch_ms", "classes"}."""
+    import torch
+
+    from .ragged import RaggedBatch
+
+    batch = RaggedBatch(items, tuning=tuning)
+    y = torch.empty_like(x)
+    ref = batch.apply(x)
+    torch.cuda.synchronize()
+    rows = []
+    for i, c in enumerate(batch.classes()):
+        idx = [k for k, it in enumerate(items) if (it[0], it[1], it[2]) == (c["h"], c["w"], c["mode"])]
+        alone = RaggedBatch([items[k] for k in idx], offsets=[int(batch.offsets[k]) for k in idx], tuning=tuning)
+        ms = {"queue": _time_graph(lambda s: alone.apply(x, y, stream=s), x, steps),
+              "launch": _time_graph(lambda s: batch.apply_class(i, "launch", x, y, stream=s), x, steps)}
+        if c["h"] * c["w"] > 16384:
+            ms["launch_small"] = _time_graph(lambda s: batch.apply_class(i, "launch_small", x, y, stream=s), x, steps)
+        best = min(ms, key=ms.get)
+        rows.append({"class": c["key"], "arrays": c["arrays"], "ms": ms, "choice": best})
+        del alone
+    chosen = {r["class"]: r["choice"] for r in rows}
+    every_launch = {r["class"]: min((k for k in r["ms"] if k != "queue"), key=r["ms"].get) for r in rows}
+    trials = []
+    for name, classes in (("per_class", chosen), ("all_launch", every_launch)):
+        for n in streams:
+            trials.append((name, {"classes": classes, "streams": int(n)}))
+    results = [("all_queue", {"classes": {}, "streams": 1}, _time_graph(lambda s: batch.apply(x, y, stream=s), x, steps))]
+    for name, sched in trials:
+        b = RaggedBatch(items, tuning=tuning, schedule=sched)
+        ms = _time_graph(lambda s: b.apply(x, y, stream=s), x, steps)
+        torch.cuda.synchronize()
+        scale = float(ref.abs().max()) or 1.0
+        if float((y - ref).abs().max()) > 1e-5 * scale:
+            raise RuntimeError(f"ragged schedule {name}/{sched['streams']} disagrees with the queue's output")
+        results.append((name, sched, ms))
+        del b
+    name, sched, ms = min(results, key=lambda r: r[2])
+    return {"schedule": sched, "kind": name, "ms": ms,
+            "queue_ms": results[0][2],
+            "trials": [{"kind": n, "streams": s["streams"], "ms": m} for n, s, m in results],
+            "classes": rows}

@@ -113,7 +113,8 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     // 2048 x 256^2 1669 -> 2129 GB/s).
     const long long nb = batch;
     cudaError_t e;
-    if (nb * (W / Gm::kTC) < 2LL * ctx.sm_count) {   // few arrays: smaller strips and row blocks
+    const bool small = nb * (W / Gm::kTC) < 2LL * ctx.sm_count || (GEN && lx.small_units);
+    if (small) {   // few arrays (or asked for): smaller strips and row blocks
       auto kcs = k_colstrip<H, W, Gm::kTCs, MODE, TC_T, GEN>;
       TileArgs ac{x, y, nb * (W / Gm::kTCs), nb * H, tab, lx, ly};
       e = launch_tiles(kcs, Gm::kSmemStripS, kernel_blocks_per_sm(kcs, Gm::kSmemStripS, TC_T), ac, ctx, st, TC_T);
@@ -122,7 +123,7 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
       e = launch_tiles(kc, Gm::kSmemStrip, bpc, ac, ctx, st, TC_T);
     }
     if (e != cudaSuccess) return e;
-    if (nb * H / Gm::kRB < 2LL * ctx.sm_count) {
+    if (nb * H / Gm::kRB < 2LL * ctx.sm_count || (GEN && lx.small_units)) {
       auto krs = k_full<H, W, Gm::kRBs, false, true, MODE, TR_T, GEN>;
       TileArgs ar{y, y, nb * H / Gm::kRBs, nb * H, tab, ly, ly};
       e = launch_tiles(krs, Gm::kSmemRowsS, kernel_blocks_per_sm(krs, Gm::kSmemRowsS, TR_T), ar, ctx, st, TR_T);

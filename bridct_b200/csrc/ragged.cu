@@ -6,11 +6,25 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/bridct_b200.h"
 #include "bridct_internal.h"
 #include "ragged.cuh"
+
+// One shape class of a ragged batch: every array of one (height, width, mode), with the device
+// table of their offsets and the schedule that runs them.
+struct RaggedClass {
+  int h = 0, w = 0, mode = 0;
+  std::vector<int> arrays;            // indices into the item list
+  long long* d_offs = nullptr;        // offsets (floats) of those arrays
+  size_t floats = 0;                  // elements of the class
+  int schedule = BRIDCT_RAGGED_QUEUE;
+};
+
+constexpr int kRaggedMaxStreams = 8;
 
 struct bridct_ragged {
   int device = 0;
@@ -27,6 +41,12 @@ struct bridct_ragged {
   unsigned spin_limit = bridct::kRaggedSpin;
   bridct_ragged_tuning tuning{};
   std::map<int, bridct_plan*> plans;    // per-array launch loop: one plan per shape
+  // shape classes, in decreasing size; classes scheduled as their own launches run on `streams`
+  // side streams forked from and joined back into the caller's stream
+  std::vector<RaggedClass> classes;
+  int streams = 4;
+  cudaStream_t aux[kRaggedMaxStreams] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[kRaggedMaxStreams] = {};
 };
 
 namespace bridct {
@@ -64,12 +84,18 @@ int block_rows(int h, int w, int budget) {
 void build_units(bridct_ragged* r) {
   const bridct_ragged_tuning& t = r->tuning;
   std::vector<int> big, small;
+  std::vector<char> queued(r->items.size(), 1);
+  for (const RaggedClass& c : r->classes)
+    if (c.schedule != BRIDCT_RAGGED_QUEUE)
+      for (int i : c.arrays) queued[i] = 0;
   r->arrays.clear();
   for (size_t i = 0; i < r->items.size(); ++i) {
     const bridct_ragged_item& it = r->items[i];
     RaggedArray a{(long long)it.offset, it.height, it.width, it.mode, 0};
     const long long e = (long long)it.height * it.width;
-    if (e <= t.tile_floats) {
+    if (!queued[i]) {
+      // run by its class's own launch: not in the queue
+    } else if (e <= t.tile_floats) {
       small.push_back((int)i);
     } else {
       a.nstrips = it.width / strip_cols(it.height, it.width, t.strip_floats);
@@ -103,6 +129,52 @@ void build_units(bridct_ragged* r) {
     if (k >= (size_t)la) rows(big[k - la]);
   }
   for (int i : small) r->units.push_back(RaggedUnit{i, UNIT_TILE, 0, 0});
+}
+
+// Groups the items into shape classes (height, width, mode), largest first, and uploads each
+// class's offset table.
+int build_classes(bridct_ragged* r) {
+  std::map<std::tuple<int, int, int>, size_t> index;
+  for (size_t i = 0; i < r->items.size(); ++i) {
+    const bridct_ragged_item& it = r->items[i];
+    const auto key = std::make_tuple(it.height, it.width, it.mode);
+    auto f = index.find(key);
+    if (f == index.end()) {
+      f = index.emplace(key, r->classes.size()).first;
+      RaggedClass c;
+      c.h = it.height;
+      c.w = it.width;
+      c.mode = it.mode;
+      r->classes.push_back(c);
+    }
+    RaggedClass& c = r->classes[f->second];
+    c.arrays.push_back((int)i);
+    c.floats += (size_t)it.height * it.width;
+  }
+  std::stable_sort(r->classes.begin(), r->classes.end(),
+                   [](const RaggedClass& a, const RaggedClass& b) { return a.floats > b.floats; });
+  for (RaggedClass& c : r->classes) {
+    std::vector<long long> offs;
+    for (int i : c.arrays) offs.push_back((long long)r->items[i].offset);
+    cudaError_t e = cudaMalloc((void**)&c.d_offs, offs.size() * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMemcpy(c.d_offs, offs.data(), offs.size() * sizeof(long long), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "ragged class tables");
+  }
+  cudaError_t e = cudaEventCreateWithFlags(&r->fork_ev, cudaEventDisableTiming);
+  for (int i = 0; e == cudaSuccess && i < kRaggedMaxStreams; ++i) {
+    e = cudaStreamCreateWithFlags(&r->aux[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->join_ev[i], cudaEventDisableTiming);
+  }
+  return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "ragged streams");
+}
+
+// One class as its own plain-form launch over the class's offset table.
+int launch_class(bridct_ragged* r, const RaggedClass& c, int schedule, const float* x, float* y, cudaStream_t st) {
+  BatchLayout l;
+  l.offs = c.d_offs;
+  l.ld = c.w;
+  l.small_units = schedule == BRIDCT_RAGGED_CLASS_LAUNCH_SMALL;
+  return launch_plain_layout(r->dev, c.h, c.w, c.mode, x, y, (long long)c.arrays.size(), &l, &l, st);
 }
 
 int upload(bridct_ragged* r) {
@@ -181,6 +253,10 @@ BRIDCT_API bridct_ragged* bridct_ragged_create_tuned(const bridct_ragged_item* i
   r->items.assign(items, items + count);
   r->span = span;
   r->tuning = t;
+  if (build_classes(r) != BRIDCT_OK) {
+    bridct_ragged_destroy(r);
+    return nullptr;
+  }
   build_units(r);
   cudaError_t e = cudaMalloc((void**)&r->d_counters, (count + 1) * sizeof(unsigned int));
   if (e == cudaSuccess) e = cudaMalloc((void**)&r->d_err, sizeof(int));
@@ -207,6 +283,12 @@ BRIDCT_API void bridct_ragged_destroy(bridct_ragged* r) {
   cudaFree(r->d_counters);
   cudaFree(r->d_err);
   for (auto& kv : r->plans) bridct_plan_destroy(kv.second);
+  for (RaggedClass& c : r->classes) cudaFree(c.d_offs);
+  for (int i = 0; i < kRaggedMaxStreams; ++i) {
+    if (r->aux[i]) cudaStreamDestroy(r->aux[i]);
+    if (r->join_ev[i]) cudaEventDestroy(r->join_ev[i]);
+  }
+  if (r->fork_ev) cudaEventDestroy(r->fork_ev);
   delete r;
 }
 
@@ -221,22 +303,98 @@ BRIDCT_API int bridct_ragged_apply_device(bridct_ragged* r, const float* x, floa
   DeviceGuard guard(r->device);
   if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(batch device)");
   cudaStream_t st = (cudaStream_t)stream;
-  cudaError_t e = cudaMemsetAsync(r->d_counters, 0, (r->items.size() + 1) * sizeof(unsigned int), st);
-  if (e != cudaSuccess) return cuda_fail(e, "ragged reset");
-  RaggedArgs args;
-  args.x = x;
-  args.y = y;
-  args.arrays = r->d_arrays;
-  args.units = r->d_units;
-  args.nunits = (int)r->units.size();
-  args.next = r->d_counters;
-  args.done = r->d_counters + 1;
-  args.err = r->d_err;
-  args.spin_limit = r->spin_limit;
-  for (int i = 0; i < 4; ++i) args.tab[i] = r->dev->fourstep[i];
-  k_ragged<<<r->grid, kRaggedThreads, kRaggedSmem, st>>>(args);
-  e = cudaGetLastError();
-  return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_ragged launch");
+  // Classes with their own launches run on side streams forked from the caller's stream (largest
+  // class first, round robin) and joined back into it; the queue's persistent kernel runs on the
+  // caller's stream meanwhile.  Capturable: the fork and join are events on captured streams.
+  std::vector<const RaggedClass*> own;
+  for (const RaggedClass& c : r->classes)
+    if (c.schedule != BRIDCT_RAGGED_QUEUE) own.push_back(&c);
+  cudaError_t e = cudaSuccess;
+  const int nst = std::max(1, std::min(r->streams, (int)own.size()));
+  if (!own.empty()) {
+    e = cudaEventRecord(r->fork_ev, st);
+    for (int i = 0; e == cudaSuccess && i < nst; ++i) e = cudaStreamWaitEvent(r->aux[i], r->fork_ev, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "ragged fork");
+    for (size_t k = 0; k < own.size(); ++k) {
+      const int s = launch_class(r, *own[k], own[k]->schedule, x, y, r->aux[k % nst]);
+      if (s) return s;
+    }
+  }
+  if (!r->units.empty()) {
+    e = cudaMemsetAsync(r->d_counters, 0, (r->items.size() + 1) * sizeof(unsigned int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "ragged reset");
+    RaggedArgs args;
+    args.x = x;
+    args.y = y;
+    args.arrays = r->d_arrays;
+    args.units = r->d_units;
+    args.nunits = (int)r->units.size();
+    args.next = r->d_counters;
+    args.done = r->d_counters + 1;
+    args.err = r->d_err;
+    args.spin_limit = r->spin_limit;
+    for (int i = 0; i < 4; ++i) args.tab[i] = r->dev->fourstep[i];
+    k_ragged<<<r->grid, kRaggedThreads, kRaggedSmem, st>>>(args);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "k_ragged launch");
+  }
+  for (int i = 0; !own.empty() && i < nst; ++i) {
+    e = cudaEventRecord(r->join_ev[i], r->aux[i]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, r->join_ev[i], 0);
+    if (e != cudaSuccess) return cuda_fail(e, "ragged join");
+  }
+  return BRIDCT_OK;
+}
+
+BRIDCT_API size_t bridct_ragged_class_count(const bridct_ragged* r) { return r ? r->classes.size() : 0; }
+
+BRIDCT_API int bridct_ragged_class_info(const bridct_ragged* r, size_t cls, int* height, int* width, int* mode,
+                                        size_t* arrays, int* schedule) {
+  if (!r || cls >= r->classes.size()) return BRIDCT_INVALID_ARGUMENT;
+  const RaggedClass& c = r->classes[cls];
+  if (height) *height = c.h;
+  if (width) *width = c.w;
+  if (mode) *mode = c.mode;
+  if (arrays) *arrays = c.arrays.size();
+  if (schedule) *schedule = c.schedule;
+  return BRIDCT_OK;
+}
+
+BRIDCT_API int bridct_ragged_set_schedule(bridct_ragged* r, const int* schedules, size_t count, int streams) {
+  if (!r || count != r->classes.size() || (count && !schedules) || streams < 1 || streams > kRaggedMaxStreams)
+    return BRIDCT_INVALID_ARGUMENT;
+  for (size_t i = 0; i < count; ++i)
+    if (schedules[i] < BRIDCT_RAGGED_QUEUE || schedules[i] > BRIDCT_RAGGED_CLASS_LAUNCH_SMALL) {
+      set_error("bridct_ragged_set_schedule: unknown schedule " + std::to_string(schedules[i]));
+      return BRIDCT_INVALID_ARGUMENT;
+    }
+  DeviceGuard guard(r->device);
+  if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(batch device)");
+  cudaError_t e = cudaDeviceSynchronize();   // the old queue may still be in use
+  if (e != cudaSuccess) return cuda_fail(e, "bridct_ragged_set_schedule");
+  for (size_t i = 0; i < count; ++i) r->classes[i].schedule = schedules[i];
+  r->streams = streams;
+  build_units(r);
+  const int s = upload(r);
+  if (s) return s;
+  const int bps = kernel_setup(reinterpret_cast<const void*>(k_ragged), kRaggedSmem, kRaggedThreads);
+  r->grid = (int)std::min<long long>((long long)r->dev->sm_count * std::max(1, bps),
+                                     std::max<size_t>(1, r->units.size()));
+  return BRIDCT_OK;
+}
+
+BRIDCT_API int bridct_ragged_apply_class_device(bridct_ragged* r, size_t cls, int schedule, const float* x, float* y,
+                                                void* stream) {
+  if (!r || !x || !y || cls >= r->classes.size() ||
+      (schedule != BRIDCT_RAGGED_CLASS_LAUNCH && schedule != BRIDCT_RAGGED_CLASS_LAUNCH_SMALL))
+    return BRIDCT_INVALID_ARGUMENT;
+  const size_t bytes = r->span * sizeof(float);
+  const uintptr_t a = (uintptr_t)x, b = (uintptr_t)y;
+  if ((a <= b ? b - a : a - b) < bytes) return BRIDCT_OVERLAPPING_BUFFERS;
+  if ((a | b) % 16) return BRIDCT_BAD_ALIGNMENT;
+  DeviceGuard guard(r->device);
+  if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(batch device)");
+  return launch_class(r, r->classes[cls], schedule, x, y, (cudaStream_t)stream);
 }
 
 BRIDCT_API int bridct_ragged_set_wait_limit(bridct_ragged* r, unsigned polls) {

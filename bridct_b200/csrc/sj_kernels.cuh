@@ -46,6 +46,7 @@ struct BatchLayout {
   const long long* offs = nullptr;
   long long bs = 0;
   long long ld = 0;
+  int small_units = 0;   // two-pass shapes: force the few-array geometry (one line group per warp)
 };
 
 struct TileArgs {

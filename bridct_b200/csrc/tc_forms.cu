@@ -6,12 +6,13 @@
 // are uploaded once per device.  Each call encodes two TMA tensor maps (input and output
 // viewed as batch x 64 FP32 matrices, box 32 x 128, 128-byte swizzle) and launches k_tc8.
 //
-// Axes of 64, 128 and 256 (any combination): two row passes of k_tcpass per batch of arrays
-// (pass 1 over rows of length W into a plan-owned scratch, pass 2 over rows of length H into
-// the output), over chunks of up to 1 GB of arrays; BF16x3 on 64x64 arrays runs both passes in
-// one launch (k_tc64) with the intermediate on chip.  The B
-// images hold C_L (or C_L^T for the inverse) split into bf16 or tf32 parts, one 64-row slice
-// per N-block, in the K-major 128-byte-swizzled layout.
+// Every other shape: two row passes of k_tcpass per batch of arrays (pass 1 over rows of length W
+// into scratch, pass 2 over rows of length H into the output), over chunks of up to 1 GB of
+// arrays; BF16x3 on 64x64 arrays runs both passes in one launch (k_tc64) with the intermediate on
+// chip.  The B images hold C_L (or C_L^T for the inverse) split into bf16 or tf32 parts, one
+// 64-row slice per N-block, in the K-major 128-byte-swizzled layout; rows of 8, 16 or 32 points
+// run as 64-float super-rows against a block-diagonal B, and the 512- and 1024-point passes stream
+// their B slices through the ring instead of keeping them resident.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -126,7 +127,7 @@ std::vector<uint8_t> b_image(int form, bool inverse) {
 
 struct TcDevice {
   void* images[3][2] = {};   // [form][inverse]
-  void* pass_images[3][3][2] = {};   // [form][log2(L) - 6][inverse], built on first use
+  void* pass_images[3][8][2] = {};   // [form][log2(points per row) - 3][inverse], built on first use
   void* fp8_images[2][2] = {};       // [L == 256][inverse]: E4M3 codes of C or C^T
   float* fp8_scales[2][2] = {};      // their 32x32 tile scales
   int* err = nullptr;
@@ -142,16 +143,21 @@ std::vector<double> dct_matrix(int L) {
 }
 
 // B image of the row pass for rows of length L: slice nb (64 output columns) at nb * kBBytes,
-// laid out [K-chunk][split][8 KB atom column]; B[n][k] = C_L[n][k] (forward) or C_L[k][n].
-template <int FORM, int L>
+// laid out [K-chunk][split][8 KB atom column]; B[n][k] = C_L[n][k] (forward) or C_L[k][n].  With
+// SUB > 1 the 64-float super-rows hold SUB rows of LS = 64 / SUB points, and B is block-diagonal:
+// SUB copies of C_LS (zeros elsewhere).
+template <int FORM, int L, int SUB = 1>
 std::vector<uint8_t> pass_image(bool inverse) {
   using PL = tc::PassLayout<FORM, L>;
   constexpr int kc_len = tc::PassForm<FORM>::kKC;
-  const std::vector<double> c = dct_matrix(L);
+  constexpr int LS = L / SUB;
+  const std::vector<double> c = dct_matrix(LS);
   std::vector<uint8_t> img((size_t)PL::kBlocks * PL::kBBytes, 0);
   for (int n = 0; n < L; ++n)
     for (int k = 0; k < L; ++k) {
-      const double v = inverse ? c[(size_t)k * L + n] : c[(size_t)n * L + k];
+      if (n / LS != k / LS) continue;   // off the diagonal blocks: zero
+      const int nn = n % LS, kk0 = k % LS;
+      const double v = inverse ? c[(size_t)kk0 * LS + nn] : c[(size_t)nn * LS + kk0];
       const int nb = n / 64, nl = n % 64, kc = k / kc_len, kk = k % kc_len;
       uint8_t* slice = &img[(size_t)nb * PL::kBBytes];
       if (FORM == tc::BF16X3) {
@@ -270,13 +276,15 @@ bool make_rows_map(CUtensorMap* m, const float* ptr, size_t rows, int L) {
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int FORM, int L>
+constexpr int lg_points(int n) { return n <= 8 ? 0 : 1 + lg_points(n / 2); }
+
+template <int FORM, int L, int SUB = 1>
 const uint4* pass_image_device(TcDevice* d, bool inverse) {
-  constexpr int li = L == 64 ? 0 : L == 128 ? 1 : 2;
+  constexpr int li = lg_points(L / SUB);
   std::lock_guard<std::mutex> lock(g_tc_mutex);
   void*& slot = d->pass_images[FORM][li][inverse ? 1 : 0];
   if (!slot) {
-    const std::vector<uint8_t> img = pass_image<FORM, L>(inverse);
+    const std::vector<uint8_t> img = pass_image<FORM, L, SUB>(inverse);
     void* ptr = nullptr;
     if (cudaMalloc(&ptr, img.size()) != cudaSuccess) return nullptr;
     if (cudaMemcpy(ptr, img.data(), img.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -288,26 +296,28 @@ const uint4* pass_image_device(TcDevice* d, bool inverse) {
   return reinterpret_cast<const uint4*>(slot);
 }
 
-// One row pass: rows x L matrix at x -> transposed arrays (R = 1 << rshift rows each) at out.
-template <int FORM, int L>
+// One row pass: rows x (L / SUB) matrix at x -> transposed arrays (R = 1 << rshift rows each) at
+// out.  SUB > 1: the rows are read as rows / SUB super-rows of L = 64 floats.
+template <int FORM, int L, int SUB = 1>
 int launch_pass(const bridct_plan* p, bool inverse, const float* x, float* out, size_t rows, int rshift,
                 cudaStream_t st, TcDevice* d) {
   using PL = tc::PassLayout<FORM, L>;
-  auto k = tc::k_tcpass<FORM, L>;
+  auto k = tc::k_tcpass<FORM, L, SUB>;
   if (kernel_setup(reinterpret_cast<const void*>(k), PL::kDynamic, tc::kPassThreads) <= 0)
     return cuda_fail(cudaErrorInvalidConfiguration, "k_tcpass shared memory");
-  const uint4* img = pass_image_device<FORM, L>(d, inverse);
+  const uint4* img = pass_image_device<FORM, L, SUB>(d, inverse);
   if (!img) return cuda_fail(cudaGetLastError(), "tensor-core coefficient upload");
+  const size_t srows = rows / SUB;   // SUB divides every array's row count (>= 8)
   CUtensorMap xm;
-  if (!make_rows_map(&xm, x, rows, L)) {
+  if (!make_rows_map(&xm, x, srows, L)) {
     set_error("cuTensorMapEncodeTiled failed");
     return BRIDCT_DEVICE_ERROR;
   }
-  const long long mtiles = (long long)((rows + tc::kRows - 1) / tc::kRows);
+  const long long mtiles = (long long)((srows + tc::kRows - 1) / tc::kRows);
   long long slots = p->dev->sm_count / PL::kBlocks;
   if (slots > mtiles) slots = mtiles;
   if (slots < 1) slots = 1;
-  k<<<(unsigned)(slots * PL::kBlocks), tc::kPassThreads, PL::kDynamic, st>>>(xm, out, img, (long long)rows, rshift,
+  k<<<(unsigned)(slots * PL::kBlocks), tc::kPassThreads, PL::kDynamic, st>>>(xm, out, img, (long long)srows, rshift,
                                                                          d->err);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_tcpass launch");
@@ -504,9 +514,14 @@ template <int FORM>
 int pass_by_length(const bridct_plan* p, int L, bool inverse, const float* x, float* out, size_t rows, int rshift,
                    cudaStream_t st, TcDevice* d) {
   switch (L) {
+    case 8: return launch_pass<FORM, 64, 8>(p, inverse, x, out, rows, rshift, st, d);
+    case 16: return launch_pass<FORM, 64, 4>(p, inverse, x, out, rows, rshift, st, d);
+    case 32: return launch_pass<FORM, 64, 2>(p, inverse, x, out, rows, rshift, st, d);
     case 64: return launch_pass<FORM, 64>(p, inverse, x, out, rows, rshift, st, d);
     case 128: return launch_pass<FORM, 128>(p, inverse, x, out, rows, rshift, st, d);
     case 256: return launch_pass<FORM, 256>(p, inverse, x, out, rows, rshift, st, d);
+    case 512: return launch_pass<FORM, 512>(p, inverse, x, out, rows, rshift, st, d);
+    case 1024: return launch_pass<FORM, 1024>(p, inverse, x, out, rows, rshift, st, d);
     default: return BRIDCT_INVALID_ARGUMENT;
   }
 }
@@ -613,13 +628,7 @@ int apply_tc_form(bridct_plan* p, int mode, int form, const float* x, float* y, 
     set_error("the FP8 form covers arrays whose axes are 128 or 256");
     return BRIDCT_INVALID_ARGUMENT;
   }
-  const bool sep_axis_h = p->h == 64 || p->h == 128 || p->h == 256;
-  const bool sep_axis_w = p->w == 64 || p->w == 128 || p->w == 256;
-  const bool kron = p->h == 8 && p->w == 8;
-  if (!kron && !(sep_axis_h && sep_axis_w)) {
-    set_error("the tensor-core forms cover 8x8 arrays and arrays whose axes are 64, 128 or 256");
-    return BRIDCT_INVALID_ARGUMENT;
-  }
+  const bool kron = p->h == 8 && p->w == 8;   // every other supported shape runs two row passes
   const size_t elems = (size_t)p->h * p->w;
   const size_t bytes = batch * elems * sizeof(float);
   const uintptr_t a = (uintptr_t)x, b = (uintptr_t)y;

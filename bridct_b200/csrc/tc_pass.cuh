@@ -1,4 +1,4 @@
-// Tensor-core precision forms for arrays with axes of 64, 128 or 256 (tcgen05 + TMEM + TMA).
+// Tensor-core precision forms for arrays of any supported shape but 8x8 (tcgen05 + TMEM + TMA).
 //
 // A 2D transform Y = C_H X C_W^T is computed as two row passes.  A row pass takes a matrix of
 // contiguous rows of length L (rows grouped into arrays of R rows), multiplies every row by
@@ -54,23 +54,40 @@ constexpr int kPassThreads = 512;
 
 constexpr int pass_min(int a, int b) { return a < b ? a : b; }
 
+// Shared-memory plan of one row pass.  The CTA's 64-column slice of C_L stays resident when it
+// fits beside a two-stage ring (L <= 256); for L = 512 and 1024 it does not (192-384 KB), and every
+// ring stage then carries the slice's K-chunk next to the A chunk (STREAM_B), brought in by a bulk
+// copy from the pre-split image in global memory (L2-resident: 0.4-1.5 MB per form and direction).
 template <int FORM, int L>
 struct PassLayout {
   using F = PassForm<FORM>;
   static constexpr int kChunks = L / F::kKC;
   static constexpr int kBlocks = L / kPassNBlock;
   static constexpr int kBBytes = F::kSplits * kChunks * kBAtom;   // this CTA's slice of C_L
+  static constexpr int kBChunk = F::kSplits * kBAtom;             // one K-chunk of the slice
   static constexpr int kABufs = 2;
   static constexpr int kBarBytes = 1024;
-  static constexpr int kFixed = kBBytes + kABufs * F::kABufBytes + kBarBytes + 1024;
-  static constexpr int kStages = pass_min(kPassMaxStages, (kPassSmemMax - kFixed) / F::kStageBytes);
+  static constexpr bool kStreamB =
+      kBBytes + kABufs * F::kABufBytes + kBarBytes + 1024 + 2 * F::kStageBytes > kPassSmemMax;
+  static constexpr int kResident = kStreamB ? 0 : kBBytes;
+  static constexpr int kStageStride = F::kStageBytes + (kStreamB ? kBChunk : 0);
+  static constexpr int kStageTx = kStageStride;                  // bytes a stage's loads deliver
+  static constexpr int kFixed = kResident + kABufs * F::kABufBytes + kBarBytes + 1024;
+  static constexpr int kStages = pass_min(kPassMaxStages, (kPassSmemMax - kFixed) / kStageStride);
   static_assert(kStages >= 2, "pass ring needs two stages");
-  static constexpr int kAOff = kStages * F::kStageBytes;
+  static constexpr int kAOff = kStages * kStageStride;
   static constexpr int kBOff = kAOff + kABufs * F::kABufBytes;
-  static constexpr int kBarOff = kBOff + kBBytes;
+  static constexpr int kBarOff = kBOff + kResident;
   static constexpr int kDynamic = kBarOff + kBarBytes + 1024;      // + 1024-byte alignment slack
   static_assert(kDynamic <= kPassSmemMax, "shared memory budget");
 };
+
+// Bulk copy of `bytes` (a multiple of 16) from global memory into shared memory, completing on bar.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
 
 struct PassBars {
   uint32_t stage_full, stage_free, a_full, a_free, acc_full, acc_free, tmem_slot;
@@ -115,16 +132,15 @@ struct PassAccs {
   __host__ __device__ static constexpr int group(int kc) { return kc * kBig / CHUNKS; }
 };
 
-// Split products of K-chunk kc (one thread).  sB: shared address of the B slice, laid out as
-// [chunk][split][8 KB atom column of 64 rows].  tmem: column 0 of this M-tile's set.
+// Split products of K-chunk kc (one thread).  bchunk: shared address of the chunk's B splits,
+// laid out [split][8 KB atom column of 64 rows].  tmem: column 0 of this M-tile's set.
 template <int FORM, int CHUNKS>
-__device__ __forceinline__ void issue_pass_mmas(uint32_t sstage, uint32_t sabuf, uint32_t sB, int kc,
+__device__ __forceinline__ void issue_pass_mmas(uint32_t sstage, uint32_t sabuf, uint32_t bchunk, int kc,
                                                 uint32_t tmem) {
   using A = PassAccs<FORM, CHUNKS>;
   const int g = A::group(kc);
   const bool big_first = kc == 0 || A::group(kc - 1) != g;
   const uint32_t big_g = tmem + A::kExtraBig + (uint32_t)(g - 1) * kPassNBlock;
-  const uint32_t bchunk = sB + (uint32_t)(kc * PassForm<FORM>::kSplits) * kBAtom;
   if constexpr (FORM == BF16X3) {
     constexpr uint32_t i192 = instr_desc(1, 192), i128 = instr_desc(1, 128), i64 = instr_desc(1, 64);
 #pragma unroll
@@ -160,10 +176,16 @@ __device__ __forceinline__ void issue_pass_mmas(uint32_t sstage, uint32_t sabuf,
 // xmap: the (nrows x L) FP32 row matrix (box 32 x 128, SWIZZLE_128B).  out: destination of
 // the transposed arrays (R rows per array, rshift = log2 R).  bimage: kBlocks slices of
 // PassLayout::kBBytes.  Grid: a multiple of kBlocks CTAs; CTA c computes N-block c % kBlocks.
-template <int FORM, int L>
+// SUB > 1 (rows of LS = 64 / SUB = 8, 16 or 32 points): L = 64 and every matrix row holds SUB
+// consecutive rows of length LS (a super-row); B is block-diagonal (SUB copies of C_LS), so
+// column n = j * LS + c of super-row g is output column c of row g * SUB + j, and nrows counts
+// super-rows.
+template <int FORM, int L, int SUB = 1>
 __global__ void __launch_bounds__(kPassThreads, 1)
     k_tcpass(const __grid_constant__ CUtensorMap xmap, float* __restrict__ out,
              const uint4* __restrict__ bimage, long long nrows, int rshift, int* __restrict__ err) {
+  static_assert(SUB == 1 || L == 64, "super-rows are 64 floats");
+  constexpr int LS = L / SUB;   // points per original row
   using PL = PassLayout<FORM, L>;
   using F = PassForm<FORM>;
   constexpr int kStages = PL::kStages;
@@ -205,7 +227,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                  "r"(ACC::kAlloc));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  {
+  if constexpr (!PL::kStreamB) {
     const uint4* src = bimage + (size_t)nblk * (PL::kBBytes / 16);
     uint4* dst = reinterpret_cast<uint4*>(base + PL::kBOff);
     for (int i = tid; i < PL::kBBytes / 16; i += kPassThreads) dst[i] = __ldg(src + i);
@@ -224,11 +246,15 @@ __global__ void __launch_bounds__(kPassThreads, 1)
       if (!ok) break;
       const long long m = slot + (j / kChunks) * nslots;
       const int kc = (int)(j % kChunks);
-      const uint32_t dst = sbase + s * F::kStageBytes;
-      mbar_expect_tx(bars.stage_full + 8 * s, F::kStageBytes);
+      const uint32_t dst = sbase + s * PL::kStageStride;
+      mbar_expect_tx(bars.stage_full + 8 * s, PL::kStageTx);
       tma_load_2d(dst, &xmap, kc * F::kKC, (int)(m * kRows), bars.stage_full + 8 * s);
       if constexpr (F::kKC == 64)
         tma_load_2d(dst + 16384u, &xmap, kc * F::kKC + 32, (int)(m * kRows), bars.stage_full + 8 * s);
+      if constexpr (PL::kStreamB)
+        bulk_load(dst + F::kStageBytes,
+                  reinterpret_cast<const uint8_t*>(bimage) + (size_t)nblk * PL::kBBytes + (size_t)kc * PL::kBChunk,
+                  PL::kBChunk, bars.stage_full + 8 * s);
     }
   } else if (warp == 1 && lane == 0) {
     for (long long j = 0; j < nchunk_local && ok && !s_abort; ++j) {
@@ -239,8 +265,11 @@ __global__ void __launch_bounds__(kPassThreads, 1)
       if (ok && kc == 0) ok = mbar_wait(bars.acc_free + 8 * t, ((uint32_t)(jt >> 1) & 1u) ^ 1u);
       if (!ok) break;
       tc_fence_after();
-      issue_pass_mmas<FORM, kChunks>(sbase + s * F::kStageBytes, sbase + PL::kAOff + a * F::kABufBytes,
-                                     sbase + PL::kBOff, kc, tmem_base + t * kTileCols);
+      const uint32_t sstage = sbase + s * PL::kStageStride;
+      const uint32_t bchunk = PL::kStreamB ? sstage + F::kStageBytes
+                                           : sbase + PL::kBOff + (uint32_t)(kc * F::kSplits) * kBAtom;
+      issue_pass_mmas<FORM, kChunks>(sstage, sbase + PL::kAOff + a * F::kABufBytes, bchunk, kc,
+                                     tmem_base + t * kTileCols);
       umma_commit(bars.stage_free + 8 * s);
       umma_commit(bars.a_free + 8 * a);
       if (kc == kChunks - 1) umma_commit(bars.acc_full + 8 * t);
@@ -265,7 +294,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         ok = r != 0;
         break;
       }
-      uint8_t* stage = base + s * F::kStageBytes;
+      uint8_t* stage = base + s * PL::kStageStride;
       uint8_t* abuf = base + PL::kAOff + a * F::kABufBytes;
       if constexpr (FORM == BF16X3) split_tile<BF16X3>(stage, abuf, r);
       else split_box_tf32(stage, abuf, r);
@@ -287,11 +316,14 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         break;
       }
       tc_fence_after();
-      // row g = (array b, row h of that array); its column n goes to out[b][n][h]
+      // row g = (array b, row h of that array); its column n goes to out[b][n][h].  With
+      // super-rows, column n = j * LS + c of super-row g goes to out[b][c][h0 + j], h0 = g * SUB
+      // within its array (SUB divides R, so a super-row lies in one array).
       const long long g = (slot + jt * nslots) * kRows + r;
       const bool live = g < nrows;
-      const long long b = g >> rshift, h = g & rmask;
-      float* dst = out + ((b * L + (long long)nblk * kPassNBlock) << rshift) + h;
+      const long long g0 = g * SUB;
+      const long long b = g0 >> rshift, h = g0 & rmask;
+      float* dst = out + ((b * LS + (long long)nblk * kPassNBlock) << rshift) + h;
       const uint32_t taddr = tmem_base + t * kTileCols + (quarter << 16);
 #pragma unroll
       for (int q = 0; q < kPassNBlock / 16; ++q) {
@@ -315,7 +347,11 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         }
         if (live) {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) dst[(long long)(q * 16 + i) << rshift] = big[i] + sm[i];
+          for (int i = 0; i < 16; ++i) {
+            constexpr int kLS = LS;
+            const int n = q * 16 + i, j = n / kLS, c = n % kLS;
+            dst[((long long)c << rshift) + j] = big[i] + sm[i];
+          }
         }
       }
       tc_fence_before();

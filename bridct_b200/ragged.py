@@ -6,9 +6,10 @@
 
 The work queue (column strips, row blocks and whole small arrays) is built once on the host;
 `apply` is one counter reset plus one kernel on torch's current stream, so it can be captured in
-a CUDA graph.  `apply_loop` runs the same batch as one plain-form launch per array, the
-comparison baseline.  The unit geometry comes from the autotuner (bridct_b200.autotune) when a
-tuning is given.
+a CUDA graph.  A schedule can instead give shape classes their own fixed-shape launches, forked
+onto side streams inside the same call (still capturable).  `apply_loop` runs the same batch as one
+plain-form launch per array, the comparison baseline.  The unit geometry and the per-class
+schedule come from the autotuner (bridct_b200.autotune).
 """
 from __future__ import annotations
 
@@ -29,9 +30,12 @@ def pack_offsets(shapes: Sequence[Tuple[int, int]]) -> Tuple[np.ndarray, int]:
     return offs, pos
 
 
+SCHEDULES = {"queue": 0, "launch": 1, "launch_small": 2}
+
+
 class RaggedBatch:
     def __init__(self, items: Iterable[Tuple[int, int, int]], offsets: Optional[Sequence[int]] = None,
-                 tuning: Optional[dict] = None):
+                 tuning: Optional[dict] = None, schedule: Optional[dict] = None):
         items = list(items)
         shapes = [(h, w) for h, w, _ in items]
         if offsets is None:
@@ -56,6 +60,8 @@ class RaggedBatch:
             self._h = L.bridct_ragged_create_tuned(arr, len(items), t)
         if not self._h:
             raise ValueError(f"bridct_ragged_create failed: {_lib.last_error()}")
+        if schedule:
+            self.set_schedule(schedule)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -70,6 +76,43 @@ class RaggedBatch:
     def units(self) -> int:
         return int(_lib.lib().bridct_ragged_units(self._h))
 
+    def classes(self) -> List[dict]:
+        """Shape classes, largest first: {"key": "HxW/mode", "h", "w", "mode", "arrays", "schedule"}."""
+        import ctypes as C
+
+        L = _lib.lib()
+        out = []
+        for i in range(int(L.bridct_ragged_class_count(self._h))):
+            h, w, m, sch = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+            n = C.c_size_t()
+            _lib.check(L.bridct_ragged_class_info(self._h, i, h, w, m, n, sch), "bridct_ragged_class_info")
+            out.append({"key": f"{h.value}x{w.value}/{m.value}", "h": h.value, "w": w.value, "mode": m.value,
+                        "arrays": int(n.value), "schedule": sch.value})
+        return out
+
+    def set_schedule(self, schedule: dict) -> None:
+        """schedule = {"classes": {"HxW/mode": "queue"|"launch"|"launch_small"}, "streams": n};
+        classes not named keep the queue."""
+        import ctypes as C
+
+        names = schedule.get("classes", {})
+        cls = self.classes()
+        arr = (C.c_int * max(1, len(cls)))()
+        for i, c in enumerate(cls):
+            v = names.get(c["key"], "queue")
+            arr[i] = SCHEDULES[v] if isinstance(v, str) else int(v)
+        _lib.check(_lib.lib().bridct_ragged_set_schedule(self._h, arr, len(cls), int(schedule.get("streams", 4))),
+                   "bridct_ragged_set_schedule")
+
+    def apply_class(self, index: int, schedule: str, x, y, stream=None):
+        """One class alone as its own launch (for measurement)."""
+        import torch
+
+        s = torch.cuda.current_stream(x.device).cuda_stream if stream is None else stream
+        _lib.check(_lib.lib().bridct_ragged_apply_class_device(self._h, index, SCHEDULES[schedule], x.data_ptr(),
+                                                               y.data_ptr(), s), "ragged class apply")
+        return y
+
     def _go(self, fn, x, y, stream):
         import torch
 
@@ -82,7 +125,8 @@ class RaggedBatch:
         return y
 
     def apply(self, x, y=None, stream=None):
-        """One persistent launch over the batch (asynchronous on the current stream)."""
+        """The whole batch: the queued classes in one persistent launch, the others as their own
+        launches on forked side streams (asynchronous on the current stream)."""
         return self._go(_lib.lib().bridct_ragged_apply_device, x, y, stream)
 
     def apply_loop(self, x, y=None, stream=None):

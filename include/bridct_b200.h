@@ -18,8 +18,8 @@ extern "C" {
 enum bridct_form {
     BRIDCT_FORM_SJ = 0,        /* FP32 Shao-Johnson CUDA-core kernels (the plan API's form); all shapes */
     BRIDCT_FORM_TC_BF16X3 = 1, /* tensor cores: 3-term bf16 split of X, 6 products, FP32 accumulation;
-                                  8x8 arrays, and arrays whose axes are 64, 128 or 256 */
-    BRIDCT_FORM_TC_TF32X3 = 2, /* tensor cores: 2-term tf32 split of X and C, 3 products; same shapes */
+                                  all shapes (8x8 as one Kronecker GEMM, the rest as two row passes) */
+    BRIDCT_FORM_TC_TF32X3 = 2, /* tensor cores: 2-term tf32 split of X and C, 3 products; all shapes */
     BRIDCT_FORM_TC_FP8 = 3     /* FP8 E4M3, per-32x32-tile scales, + one FP32 refinement step;
                                   arrays whose axes are 128 or 256 */
 };
@@ -71,7 +71,7 @@ BRIDCT_API int bridct_plan_apply_strided_device(bridct_plan *plan, enum bridct_m
 
 /* As bridct_plan_apply_device, with an explicit execution form (precision forms run
  * on the tensor cores; see enum bridct_form for the shapes each form supports).  The
- * tensor-core forms on axes of 64..256 and the FP8 form keep their intermediate in scratch
+ * two-pass tensor-core forms and the FP8 form keep their intermediate in scratch
  * owned by the plan (allocated by the first call that needs it, so make that call before any
  * stream capture): calls on one plan must not run concurrently on different streams.  The
  * scratch holds one chunk of the batch and grows with the largest batch a plan has seen: up
@@ -142,10 +142,38 @@ BRIDCT_API bridct_ragged *bridct_ragged_create_tuned(const bridct_ragged_item *i
                                                      const bridct_ragged_tuning *tuning);
 BRIDCT_API void bridct_ragged_destroy(bridct_ragged *batch);
 BRIDCT_API size_t bridct_ragged_units(const bridct_ragged *batch);
-/* One persistent launch over the whole batch (device pointers, asynchronous on `stream`,
- * capturable in a CUDA graph: a counter reset and one kernel). */
+/* Runs the whole batch (device pointers, asynchronous on `stream`, capturable in a CUDA graph):
+ * the arrays of classes scheduled BRIDCT_RAGGED_QUEUE in one persistent launch (a counter reset and
+ * one kernel), and every other class as its own launch on side streams forked from `stream` and
+ * joined back into it.  A new batch schedules every class on the queue. */
 BRIDCT_API int bridct_ragged_apply_device(bridct_ragged *batch, const float *input, float *output,
                                           void *stream);
+
+/* ---- Per-shape-class schedules of a ragged batch ----------------------------------------------
+ * The batch's arrays fall into shape classes (height, width, mode), numbered largest first (by
+ * elements).  Each class runs either in the shared persistent queue, or as its own launch of the
+ * fixed-shape kernels of that shape over the class's offset table, with the tile shapes measured
+ * best for that shape, or with the few-array geometry (one four-step line group per warp).  The
+ * autotuner (bridct_b200.autotune) measures the choices per class.  No reference counterpart: the
+ * reference picks a per-(h, w, mode) policy from a table (src/generated/rect_policy.inc,
+ * src/plan.c:140-148). */
+enum bridct_ragged_schedule {
+    BRIDCT_RAGGED_QUEUE = 0,               /* units in the persistent kernel's queue           */
+    BRIDCT_RAGGED_CLASS_LAUNCH = 1,        /* the class's own fixed-shape launch               */
+    BRIDCT_RAGGED_CLASS_LAUNCH_SMALL = 2   /* the same with the few-array geometry (two-pass)  */
+};
+BRIDCT_API size_t bridct_ragged_class_count(const bridct_ragged *batch);
+/* Shape, mode, array count and schedule of class `cls` (any output pointer may be NULL). */
+BRIDCT_API int bridct_ragged_class_info(const bridct_ragged *batch, size_t cls, int *height, int *width,
+                                        int *mode, size_t *arrays, int *schedule);
+/* Sets every class's schedule (count = bridct_ragged_class_count) and the number of side streams
+ * (1..8) that own launches spread over.  Rebuilds the queue: synchronizes the device and may
+ * allocate, so call it outside stream capture and before capturing the batch's launches. */
+BRIDCT_API int bridct_ragged_set_schedule(bridct_ragged *batch, const int *schedules, size_t count,
+                                          int streams);
+/* One class alone as its own launch (schedule CLASS_LAUNCH or CLASS_LAUNCH_SMALL), for measuring. */
+BRIDCT_API int bridct_ragged_apply_class_device(bridct_ragged *batch, size_t cls, int schedule,
+                                                const float *input, float *output, void *stream);
 /* The same batch as one plain-form launch per array (the comparison baseline). */
 BRIDCT_API int bridct_ragged_apply_loop_device(bridct_ragged *batch, const float *input,
                                                float *output, void *stream);

@@ -144,3 +144,91 @@ def test_ragged_dependency_wait_expires_and_reports():
     for (h, w, m), xi, yi in zip(items, b.unpack(x), b.unpack(y)):
         xi, yi = xi.cpu().numpy(), yi.cpu().numpy()
         assert O.rel_max_error(yi, O.fp64_apply(xi, m), xi, output_scaled=True) <= TOL, (h, w, m)
+
+
+def _all(b, kind):
+    return {c["key"]: kind for c in b.classes()}
+
+
+@pytest.mark.parametrize("kind,streams", [("launch", 1), ("launch", 4), ("launch_small", 8), ("mixed", 3)])
+def test_class_schedules_match_the_queue_and_fp64(kind, streams):
+    items = random_batch(200, 11)
+    items += [(1024, 1024, 0), (1024, 1024, 1), (512, 256, 2), (8, 8, 0), (8, 8, 1)]
+    b = RaggedBatch(items)
+    rng = np.random.default_rng(12)
+    x = torch.from_numpy(rng.uniform(-1, 1, b.span).astype(np.float32)).cuda()
+    ref = b.apply(x)
+    torch.cuda.synchronize()
+    classes = b.classes()
+    assert sum(c["arrays"] for c in classes) == len(items)
+    assert [c["h"] * c["w"] * c["arrays"] for c in classes] == sorted(
+        (c["h"] * c["w"] * c["arrays"] for c in classes), reverse=True)
+    if kind == "mixed":
+        sched = {c["key"]: ("queue", "launch", "launch_small")[i % 3] for i, c in enumerate(classes)}
+    else:
+        sched = _all(b, kind)
+    s = RaggedBatch(items, schedule={"classes": sched, "streams": streams})
+    assert all(c["schedule"] == {"queue": 0, "launch": 1, "launch_small": 2}[sched[c["key"]]] for c in s.classes())
+    y = s.apply(x)
+    torch.cuda.synchronize()
+    assert not s.timed_out()
+    close(y, ref, x, items, b)
+    for i in range(0, len(items), 17):
+        h, w, m = items[i]
+        xi, yi = b.unpack(x)[i].cpu().numpy(), b.unpack(y)[i].cpu().numpy()
+        assert O.rel_max_error(yi, O.fp64_apply(xi, m), xi, output_scaled=True) <= TOL, (h, w, m)
+
+
+def test_class_schedule_graph_capture_and_replay():
+    items = random_batch(96, 13)
+    b = RaggedBatch(items)
+    b.set_schedule({"classes": {c["key"]: ("launch" if i % 2 else "queue") for i, c in enumerate(b.classes())},
+                    "streams": 4})
+    x = torch.randn(b.span, device="cuda")
+    y = torch.empty_like(x)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        b.apply(x, y, stream=s.cuda_stream)
+    s.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        b.apply(x, y, stream=s.cuda_stream)
+    y.zero_()
+    with torch.cuda.stream(s):
+        g.replay()
+    s.synchronize()
+    ref = RaggedBatch(items).apply(x)
+    torch.cuda.synchronize()
+    close(y, ref, x, items, b)
+
+
+def test_class_schedule_rejects_bad_arguments():
+    from bridct_b200 import _lib
+    import ctypes as C
+
+    b = RaggedBatch(random_batch(20, 2))
+    n = len(b.classes())
+    arr = (C.c_int * n)(*([1] * n))
+    L = _lib.lib()
+    assert L.bridct_ragged_set_schedule(b._h, arr, n + 1, 4) == _lib.INVALID_ARGUMENT
+    assert L.bridct_ragged_set_schedule(b._h, arr, n, 9) == _lib.INVALID_ARGUMENT
+    bad = (C.c_int * n)(*([3] * n))
+    assert L.bridct_ragged_set_schedule(b._h, bad, n, 4) == _lib.INVALID_ARGUMENT
+    x = torch.zeros(b.span, device="cuda")
+    assert L.bridct_ragged_apply_class_device(b._h, 0, 0, x.data_ptr(), x.data_ptr(), None) == _lib.INVALID_ARGUMENT
+    assert L.bridct_ragged_apply_class_device(b._h, n, 1, x.data_ptr(), x.data_ptr(), None) == _lib.INVALID_ARGUMENT
+
+
+def test_tune_classes_returns_a_checked_schedule():
+    from bridct_b200.autotune import tune_classes
+
+    items = random_batch(40, 17, max_elems=1 << 18)
+    x = torch.randn(RaggedBatch(items).span, device="cuda")
+    res = tune_classes(items, x, steps=2, streams=(1, 4))
+    assert res["ms"] <= res["queue_ms"]
+    assert len(res["classes"]) == len(RaggedBatch(items).classes())
+    b = RaggedBatch(items, schedule=res["schedule"])
+    got = b.apply(x)
+    ref = RaggedBatch(items).apply(x)
+    torch.cuda.synchronize()
+    close(got, ref, x, items, b)

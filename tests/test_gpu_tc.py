@@ -1,5 +1,6 @@
 """Tensor-core precision forms (tcgen05/TMEM/TMA) against float64: the Kronecker form for 8x8
-batches and the two-pass separable form for arrays whose axes are 64, 128 or 256.
+batches and the two-pass separable form for every other shape (axes of 8..32 as block-diagonal
+64-float super-rows, 512 and 1024 with the coefficient slice streamed through the ring).
 
 Tolerance: max|y - y64| / max(max|x|, max|y64|) <= 2e-6 per array, the same bound as the
 plain form; the literal max|x| form of the bound is checked on the block-image data.
@@ -67,13 +68,13 @@ def test_tc8_no_write_past_batch(form):
     assert torch.isfinite(y[:300]).all()
 
 
-@pytest.mark.parametrize("shape", [(16, 16), (32, 64), (512, 512), (8, 64)])
-def test_tc_forms_reject_other_shapes(shape):
+@pytest.mark.parametrize("shape", [(16, 16), (32, 64), (512, 512), (8, 64), (1024, 128)])
+def test_fp8_form_rejects_other_shapes(shape):
     L = _lib.lib()
     plan = torch_api._plan(torch.cuda.current_device(), *shape)
     x = torch.randn(4, *shape, device="cuda")
     y = torch.empty_like(x)
-    st = L.bridct_plan_apply_form_device(plan, 0, _lib.FORM_TC_BF16X3, x.data_ptr(), y.data_ptr(), 4, None)
+    st = L.bridct_plan_apply_form_device(plan, 0, _lib.FORM_TC_FP8, x.data_ptr(), y.data_ptr(), 4, None)
     assert st == _lib.INVALID_ARGUMENT
 
 
@@ -214,3 +215,61 @@ def test_fp8_batch_across_chunks_matches_small_batches_bitwise():
     part = torch_api.apply(x[2044:2052].clone(), 0, form="tc_fp8")
     torch.cuda.synchronize()
     assert torch.equal(y[2044:2052], part)
+
+
+ALL_SHAPES = [(h, w) for h in (8, 16, 32, 64, 128, 256, 512, 1024) for w in (8, 16, 32, 64, 128, 256, 512, 1024)
+              if (h, w) != (8, 8)]
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("shape", ALL_SHAPES)
+def test_tc_every_shape_matches_fp64(form, shape):
+    h, w = shape
+    batch = 2 if h * w >= 262144 else 3 if h * w >= 16384 else 37   # partial 128-row tiles
+    x = np.random.default_rng(h * 3 + w).uniform(-1, 1, (batch, h, w)).astype(np.float32)
+    for mode in range(3):
+        y = run(x, mode, form)
+        ref = O.fp64_apply(x, mode)
+        assert O.rel_max_error(y, ref, x, output_scaled=True) <= sep_tol(form, mode), (form, shape, mode)
+
+
+def large_arrays():
+    """The large-array configuration: N(0,1) plus sin(2 pi x / 97) cos(2 pi y / 61) (seed 2)."""
+    rng = np.random.default_rng(2)
+    out = []
+    for h, w in ((1024, 1024), (1024, 512), (512, 1024)):
+        yy, xx = np.mgrid[0:h, 0:w]
+        out.append((rng.standard_normal((h, w)) + np.sin(2 * np.pi * xx / 97) * np.cos(2 * np.pi * yy / 61))
+                   .astype(np.float32)[None])
+    return out
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_tc_large_arrays_against_fp64_and_the_plain_form(form):
+    """Config 3's comparison: the tensor-core forms on 1024^2, 1024x512 and 512x1024 arrays in every
+    mode, against float64 (output-scaled bound) and beside the plain SJ form."""
+    for x in large_arrays():
+        for mode in range(3):
+            y = run(x, mode, form)
+            ref = O.fp64_apply(x, mode)
+            e = O.rel_max_error(y, ref, x, output_scaled=True)
+            assert e <= sep_tol(form, mode), (form, x.shape, mode, e)
+            sj = run(x, mode, "sj")
+            assert O.rel_max_error(y, sj, x, output_scaled=True) <= 2 * sep_tol(form, mode)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_tc_golden_config_samples(form):
+    """The reference library's own outputs on the committed samples of the benchmark
+    configurations (64x64, 8x8 blocks, 64x128 N(0,1)+smooth, 256x256 log-uniform)."""
+    from tests.helpers import golden
+
+    g = golden("configs.npz")
+    keys = sorted(k for k in g.files if k.endswith("_x"))
+    assert len(keys) == 4
+    for k in keys:
+        x = g[k]
+        for mode in range(3):
+            y = run(x, mode, form)
+            ref = g[k[:-2] + f"_y{mode}"]
+            assert O.rel_max_error(y, ref, x, output_scaled=True) <= 2 * sep_tol(form, mode), (k, mode)
