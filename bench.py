@@ -884,9 +884,9 @@ def shard_of(x, rank: int, world: int):
     from bridct_b200.dist import shard_range
 
     b = x.shape[0]
-    first, count = shard_range(b * world, rank, world)
     if world == 1:
         return x, 0
+    first, count = shard_range(b * world, rank, world)
     return np.ascontiguousarray(x[np.arange(first, first + count) % b]), first
 
 

@@ -22,6 +22,26 @@ static int kernel_blocks_per_sm(Kernel k, int smem, int threads = kThreads) {
   return kernel_setup(reinterpret_cast<const void*>(k), smem, threads);
 }
 
+// Launches a plain-form kernel with programmatic stream serialization (see griddep_wait): its
+// CTAs may be scheduled, and run up to their first global access, while the previous kernel in
+// the stream finishes, which hides most of the launch gap between back-to-back launches (the two
+// passes of a two-pass shape, or consecutive calls).
+template <typename... Params, typename... Args>
+static cudaError_t launch_pdl(void (*k)(Params...), unsigned grid, unsigned threads, int smem, cudaStream_t st,
+                              Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = (size_t)smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <typename Kernel>
 static cudaError_t launch_tiles(Kernel k, int smem, int bps, TileArgs a, const LaunchCtx& ctx,
                                 cudaStream_t st, int threads = kThreads) {
@@ -29,8 +49,7 @@ static cudaError_t launch_tiles(Kernel k, int smem, int bps, TileArgs a, const L
   if (a.ntiles <= 0) return cudaSuccess;
   long long grid = (long long)ctx.sm_count * bps;
   if (grid > a.ntiles) grid = a.ntiles;
-  k<<<(unsigned)grid, threads, smem, st>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k, (unsigned)grid, (unsigned)threads, smem, st, a);
 }
 
 // GEN: the batch has general layouts (strided arrays or an offset table, BatchLayout); the same
@@ -56,8 +75,7 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
       const long long ntiles = (batch + kB8dbThreads - 1) / kB8dbThreads;
       long long grid = (long long)ctx.sm_count * bps;
       if (grid > ntiles) grid = ntiles;
-      k<<<(unsigned)grid, kB8dbThreads, smem, st>>>(x, y, batch);
-      return cudaGetLastError();
+      return launch_pdl(k, (unsigned)grid, kB8dbThreads, smem, st, x, y, batch);
     }
     auto k = k_blocks8<MODE>;
     constexpr int smem = kB8Chunks * 16;
@@ -66,8 +84,7 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     const long long ntiles = (batch + kB8Threads - 1) / kB8Threads;
     long long grid = (long long)ctx.sm_count * bps;
     if (grid > ntiles) grid = ntiles;
-    k<<<(unsigned)grid, kB8Threads, smem, st>>>(x, y, batch);
-    return cudaGetLastError();
+    return launch_pdl(k, (unsigned)grid, kB8Threads, smem, st, x, y, batch);
   } else if constexpr (Gm::kTile) {
     // 16384-float tiles instead of 8192 where they measured faster on 128 MiB batches: 64-wide
     // arrays up to 64 high (+6..14%, except the 64 x 64 inverse, -2%) and forward/inverse of

@@ -58,7 +58,9 @@ __global__ void __launch_bounds__(kB8Threads) k_blocks8(const float* __restrict_
   const long long rest = batch - full * round_arrays;
   const long long per = rest / gridDim.x, extra = rest % gridDim.x;
   const int t = threadIdx.x;
+  griddep_wait();
   for (long long round = 0; round <= full; ++round) {
+    if (round == full) griddep_trigger();
     long long first;
     int arrays;
     if (round < full) {
@@ -145,9 +147,12 @@ __global__ void __launch_bounds__(kB8dbThreads) k_blocks8_db(const float* __rest
       if (q < arrays * 16) b8_cp_async16(buf + b8_slot(q), src + q);
     }
   };
+  griddep_wait();
   if (nrounds > 0) issue(0);
   asm volatile("cp.async.commit_group;" ::: "memory");
+  if (nrounds <= 1) griddep_trigger();
   for (long long round = 0; round < nrounds; ++round) {
+    if (round + 1 == nrounds - 1) griddep_trigger();   // the last round's loads are being issued
     if (round + 1 < nrounds) issue(round + 1);
     asm volatile("cp.async.commit_group;" ::: "memory");
     asm volatile("cp.async.wait_group 1;" ::: "memory");   // this round's copies have landed

@@ -317,6 +317,7 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
   float* tile = smem;
   float* xbuf = smem + round4(TR * P);
   float* tabs = xbuf + round4(XB);
+  griddep_wait();
   const FourStepTables tcol = DO_COL ? stage_tables<H>(a.tab.col, tabs) : a.tab.col;
   const FourStepTables trow = DO_ROW ? stage_tables<W>(a.tab.row, tabs + (DO_COL ? TableFloats<H>::value : 0))
                                      : a.tab.row;
@@ -347,6 +348,7 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
     else next.load(a.x + blockIdx.x * (long long)TR * W, W, rows_of(blockIdx.x));
   }
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    if (t + gridDim.x >= a.ntiles) griddep_trigger();   // this CTA's last tile
     const int rows = rows_of(t);
     if constexpr (kPrefetch) {
       next.put(tile);
@@ -385,6 +387,7 @@ __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
   extern __shared__ float smem[];
   float* tile = smem;
   float* xbuf = smem + round4(H * P);
+  griddep_wait();
   const FourStepTables tcol = stage_tables<H>(a.tab.col, xbuf + round4((THREADS / 32) * ExchangeFloats<H>::value));
   // Strips of 128- and 256-point columns prefetch the next strip into registers during the
   // transform; longer columns keep their occupancy.
@@ -396,6 +399,7 @@ __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
   TileRegs<P, kPrefetch ? H : 4, kPrefetch ? TC : 4, THREADS> next;
   if (kPrefetch && blockIdx.x < a.ntiles) next.load(src(blockIdx.x), xp, H);
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    if (t + gridDim.x >= a.ntiles) griddep_trigger();   // this CTA's last strip
     const long long arr = t / STRIPS;
     const int s = (int)(t % STRIPS);
     if constexpr (kPrefetch) {

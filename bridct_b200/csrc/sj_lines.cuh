@@ -30,6 +30,15 @@ namespace bridct {
 
 enum LineMode { LM_FWD = 0, LM_INV = 1, LM_RT = 2 };
 
+// Programmatic dependent launch: the plain kernels are launched with programmatic stream
+// serialization, so a kernel's CTAs may be scheduled while the previous kernel in the stream is
+// still finishing.  griddep_wait() blocks until every prerequisite grid has completed and its
+// memory is visible; each kernel calls it before its first global access, so results are exactly
+// those of a serialized launch (without a prerequisite it returns at once).  griddep_trigger()
+// lets the next kernel's CTAs be scheduled once every CTA of this one has reached it.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---------------------------------------------------------------------------------------
 // Register lines (N <= 128; the fixed-shape kernels use them for N = 128, the ragged kernel
 // only up to 64)

@@ -120,24 +120,30 @@ __device__ __forceinline__ void split_box_tf32(uint8_t* stage, uint8_t* abuf, ui
 //   TF32x3 blocks [big0 | small | big1 | big2]:
 //     Xh.[Ch|Cl] -> [big0|small] (group 0) or Xh.Ch -> big_g, Xh.Cl -> small;  Xl.Ch -> small
 // The epilogue adds the blocks in FP32.
-template <int FORM, int CHUNKS>
+// SETS accumulator sets share the 512 TMEM columns: two (the epilogue of one M-tile overlaps the
+// MMAs of the next) for rows up to 256 points, one for 512- and 1024-point rows, whose long K
+// needs more group accumulators than two sets leave room for (TF32x3 round trips of 1024-point
+// axes exceeded 3e-6 with three groups; one set holds seven for TF32x3, six for BF16x3).
+template <int FORM, int CHUNKS, int SETS = 2>
 struct PassAccs {
-  static constexpr int kMaxBig = FORM == BF16X3 ? 2 : 3;
-  static constexpr int kBig = CHUNKS < kMaxBig ? CHUNKS : kMaxBig;
   static constexpr int kSmallBlocks = FORM == BF16X3 ? 2 : 1;
+  static constexpr int kMaxBig = SETS == 2 ? (FORM == BF16X3 ? 2 : 3) : 512 / kPassNBlock - kSmallBlocks;
+  static constexpr int kBig = CHUNKS < kMaxBig ? CHUNKS : kMaxBig;
   static constexpr int kPerTile = (1 + kSmallBlocks + (kBig - 1)) * kPassNBlock;   // columns
   static constexpr int kExtraBig = (1 + kSmallBlocks) * kPassNBlock;               // big1 column
-  static constexpr int kAlloc = 2 * kPerTile <= 256 ? 256 : 512;
-  static_assert(2 * kPerTile <= 512, "TMEM columns");
+  static constexpr int kAlloc = SETS * kPerTile <= 256 ? 256 : 512;
+  static_assert(SETS * kPerTile <= 512, "TMEM columns");
   __host__ __device__ static constexpr int group(int kc) { return kc * kBig / CHUNKS; }
 };
 
+template <int L> struct PassSets { static constexpr int value = L >= 512 ? 1 : 2; };
+
 // Split products of K-chunk kc (one thread).  bchunk: shared address of the chunk's B splits,
 // laid out [split][8 KB atom column of 64 rows].  tmem: column 0 of this M-tile's set.
-template <int FORM, int CHUNKS>
+template <int FORM, int CHUNKS, int SETS>
 __device__ __forceinline__ void issue_pass_mmas(uint32_t sstage, uint32_t sabuf, uint32_t bchunk, int kc,
                                                 uint32_t tmem) {
-  using A = PassAccs<FORM, CHUNKS>;
+  using A = PassAccs<FORM, CHUNKS, SETS>;
   const int g = A::group(kc);
   const bool big_first = kc == 0 || A::group(kc - 1) != g;
   const uint32_t big_g = tmem + A::kExtraBig + (uint32_t)(g - 1) * kPassNBlock;
@@ -190,7 +196,8 @@ __global__ void __launch_bounds__(kPassThreads, 1)
   using F = PassForm<FORM>;
   constexpr int kStages = PL::kStages;
   constexpr int kChunks = PL::kChunks;
-  using ACC = PassAccs<FORM, kChunks>;
+  constexpr int kSets = PassSets<L>::value;
+  using ACC = PassAccs<FORM, kChunks, kSets>;
   constexpr uint32_t kTileCols = ACC::kPerTile;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -260,15 +267,15 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     for (long long j = 0; j < nchunk_local && ok && !s_abort; ++j) {
       const int s = (int)(j % kStages), a = (int)(j & 1);
       const long long jt = j / kChunks;
-      const int kc = (int)(j % kChunks), t = (int)(jt & 1);
+      const int kc = (int)(j % kChunks), t = (int)(jt % kSets);
       ok = mbar_wait(bars.a_full + 8 * a, (uint32_t)(j >> 1) & 1u);
-      if (ok && kc == 0) ok = mbar_wait(bars.acc_free + 8 * t, ((uint32_t)(jt >> 1) & 1u) ^ 1u);
+      if (ok && kc == 0) ok = mbar_wait(bars.acc_free + 8 * t, ((uint32_t)(jt / kSets) & 1u) ^ 1u);
       if (!ok) break;
       tc_fence_after();
       const uint32_t sstage = sbase + s * PL::kStageStride;
       const uint32_t bchunk = PL::kStreamB ? sstage + F::kStageBytes
                                            : sbase + PL::kBOff + (uint32_t)(kc * F::kSplits) * kBAtom;
-      issue_pass_mmas<FORM, kChunks>(sstage, sbase + PL::kAOff + a * F::kABufBytes, bchunk, kc,
+      issue_pass_mmas<FORM, kChunks, kSets>(sstage, sbase + PL::kAOff + a * F::kABufBytes, bchunk, kc,
                                      tmem_base + t * kTileCols);
       umma_commit(bars.stage_free + 8 * s);
       umma_commit(bars.a_free + 8 * a);
@@ -307,9 +314,9 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     const uint32_t quarter = (uint32_t)(warp & 3) * 32u;
     const long long rmask = (1ll << rshift) - 1;
     for (long long jt = 0; jt < ntile_local; ++jt) {
-      const int t = (int)(jt & 1);
+      const int t = (int)(jt % kSets);
       if (r == 0)
-        s_group_ok[1] = (!s_abort && mbar_wait(bars.acc_full + 8 * t, (uint32_t)(jt >> 1) & 1u)) ? 1 : 0;
+        s_group_ok[1] = (!s_abort && mbar_wait(bars.acc_full + 8 * t, (uint32_t)(jt / kSets) & 1u)) ? 1 : 0;
       named_sync(2, 128);
       if (!s_group_ok[1]) {
         ok = r != 0;

@@ -1,12 +1,18 @@
 """Multi-GPU plumbing for batches of independent arrays.
 
-Every array is an independent unit, so a batch shards across ranks with no exchange step: each
-rank transforms its own slice on its own GPU and no collective touches the data.  The only
-collective is the timing reduction (max over ranks of a device-measured duration).
+Every array is an independent unit, so a batch shards across ranks (or across the devices of one
+process) with no exchange step: each shard is transformed on its own GPU and no collective touches
+the data.  The only collective in a timed run is the timing reduction (max over ranks of a
+device-measured duration).
+
+    first, count = shard_range(batch, rank, world)     # this rank's contiguous slice
+    mine, first = shard(x, rank, world)                 # the slice itself (a view)
+    y = apply_sharded(x, mode, devices=[0, 1, 2, 3])    # one process driving several GPUs
+    full = gather_shards(y_mine, first, batch)          # tests / callers that want one array back
 """
 from __future__ import annotations
 
-from typing import Tuple
+from typing import Callable, List, Optional, Sequence, Tuple
 
 
 def shard_range(batch: int, rank: int, world: int) -> Tuple[int, int]:
@@ -16,6 +22,92 @@ def shard_range(batch: int, rank: int, world: int) -> Tuple[int, int]:
     base, extra = divmod(batch, world)
     first = rank * base + min(rank, extra)
     return first, base + (1 if rank < extra else 0)
+
+
+def shard(x, rank: int, world: int):
+    """Rank's contiguous slice of the arrays in x (leading axis) and its first index."""
+    first, count = shard_range(int(x.shape[0]), rank, world)
+    return x[first:first + count], first
+
+
+def stitch(parts: Sequence[Tuple[int, object]], batch: int):
+    """Concatenates (first, shard) pieces in order after checking that they tile [0, batch)."""
+    import numpy as np
+
+    parts = sorted(parts, key=lambda p: p[0])
+    pos = 0
+    for first, piece in parts:
+        if first != pos:
+            raise ValueError(f"shards do not tile the batch: expected first {pos}, got {first}")
+        pos += int(piece.shape[0])
+    if pos != batch:
+        raise ValueError(f"shards cover {pos} of {batch} arrays")
+    pieces = [p for _, p in parts]
+    if pieces and hasattr(pieces[0], "cpu"):
+        import torch
+
+        return torch.cat([p.cpu() for p in pieces])
+    return np.concatenate(pieces) if pieces else np.empty((0,))
+
+
+def apply_sharded(x, mode: int, devices: Optional[Sequence[int]] = None, form: str = "sj",
+                  transform: Optional[Callable] = None):
+    """Transforms a batch (numpy array or tensor, (B, h, w)) split over several GPUs of this
+    process: shard i goes to devices[i], each device runs its shard on its own current stream with
+    its own cached plan, and the results come back stitched in order (a tensor on the input's
+    device for tensor input, a numpy array for numpy input).  No collective is involved.
+
+    `transform(piece, mode, device)` replaces the per-device transform (the default moves the
+    shard to the device and runs bridct_b200.torch_api.apply)."""
+    import numpy as np
+
+    if devices is None:
+        import torch
+
+        devices = list(range(torch.cuda.device_count()))
+    if not devices:
+        raise ValueError("apply_sharded needs at least one device")
+    if transform is None:
+        transform = _device_transform(form)
+    world = len(devices)
+    outs: List[Tuple[int, object]] = []
+    for r, dev in enumerate(devices):
+        piece, first = shard(x, r, world)
+        if int(piece.shape[0]):
+            outs.append((first, transform(piece, mode, dev)))
+    full = stitch(outs, int(x.shape[0]))
+    if isinstance(x, np.ndarray):
+        return full.numpy() if hasattr(full, "numpy") else full
+    return full.to(x.device) if hasattr(x, "device") else full
+
+
+def _device_transform(form: str):
+    def run(piece, mode, dev):
+        import numpy as np
+        import torch
+
+        from . import torch_api
+
+        t = torch.from_numpy(np.ascontiguousarray(piece)) if isinstance(piece, np.ndarray) else piece
+        with torch.cuda.device(dev):
+            y = torch_api.apply(t.to(f"cuda:{dev}", non_blocking=True), mode, form=form)
+        return y
+
+    return run
+
+
+def gather_shards(local, first: int, batch: int):
+    """Rank 0 receives every rank's (first, shard) over the default process group and returns the
+    stitched batch; other ranks return None.  For checking and collecting results, not for the
+    timed data path."""
+    import torch.distributed as dist
+
+    world = dist.get_world_size()
+    items = [None] * world
+    dist.all_gather_object(items, (first, local))
+    if dist.get_rank() != 0:
+        return None
+    return stitch(items, batch)
 
 
 def max_over_ranks(value, device=None):

@@ -196,3 +196,30 @@ def test_gpu_route_labels():
         p = L.bridct_plan_create(h, w)
         assert L.bridct_plan_gpu_route(p).decode() == want
         L.bridct_plan_destroy(p)
+
+
+@pytest.mark.parametrize("shape", [(262144, 8, 8), (100, 64, 64), (3, 1024, 1024), (7, 256, 512), (5, 64, 512)])
+def test_back_to_back_dependent_launches(shape):
+    """Each call reads the previous call's output on the same stream with no host synchronization
+    in between (the plain kernels overlap their start with the previous kernel's end and wait for
+    its results before their first global access): the chain forward, inverse, forward, inverse
+    returns the input, and every intermediate equals the same call made alone."""
+    import torch
+
+    from bridct_b200 import torch_api
+
+    x = torch.randn(*shape, device="cuda")
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        a = torch_api.apply(x, 0)
+        b = torch_api.apply(a, 1)
+        c = torch_api.apply(b, 0)
+        d = torch_api.apply(c, 1)
+    s.synchronize()
+    ref_a = torch_api.apply(x, 0)
+    torch.cuda.synchronize()
+    assert torch.equal(a, ref_a)
+    assert torch.equal(c, torch_api.apply(b, 0))
+    tol = 8e-6 * float(x.abs().max())
+    assert float((d - x).abs().max()) <= tol

@@ -81,3 +81,18 @@ def test_calls_leave_the_current_device_unchanged():
     torch_api.apply(x, 0, form="tc_bf16x3")
     torch.cuda.synchronize()
     assert torch.cuda.current_device() == dev
+
+
+def test_apply_sharded_over_the_visible_devices():
+    """One process splitting a batch over every visible GPU (each shard on its own device) gives
+    the single-call result."""
+    from bridct_b200.dist import apply_sharded
+
+    x = torch.randn(13, 64, 128, device="cuda")
+    devs = list(range(torch.cuda.device_count())) * 2       # with one GPU: two shards on it
+    y = apply_sharded(x, 0, devices=devs)
+    assert torch.equal(y, torch_api.apply(x, 0))
+    xn = x.cpu().numpy()
+    yn = apply_sharded(xn, 1, devices=devs)
+    assert isinstance(yn, np.ndarray)
+    assert O.rel_max_error(yn, O.fp64_apply(xn, 1), xn, True) <= TOL

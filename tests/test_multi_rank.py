@@ -1,12 +1,14 @@
 """Host-side multi-rank logic on CPU: two gloo ranks partition a batch with no overlap and no
-data collective, and agree on the max-over-ranks timing."""
+data collective, agree on the max-over-ranks timing, and, transforming their own shards (with the
+oracle standing in for each rank's GPU), stitch back exactly the full-batch result.  The same
+partition (bridct_b200.dist.shard / shard_range) feeds bench.py --gpus N and apply_sharded."""
 import os
 import socket
 
 import pytest
 import torch.multiprocessing as mp
 
-from bridct_b200.dist import max_over_ranks, shard_range
+from bridct_b200.dist import apply_sharded, gather_shards, max_over_ranks, shard, shard_range, stitch
 
 
 def test_shard_range_covers_batch():
@@ -61,3 +63,65 @@ def test_two_gloo_ranks():
     assert [r[1:3] for r in res] == [(0, 500), (500, 500)]
     assert sum(r[3] for r in res) == sum(range(1000))
     assert all(r[4] == 2.0 for r in res)
+
+
+def _transform_worker(rank, world, port, q):
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+
+    from oracle import oracle as O
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        job = np.random.default_rng(5).uniform(-1, 1, (37, 16, 32)).astype(np.float32)  # every rank builds the job
+        mine, first = shard(job, rank, world)                   # and transforms only its own arrays
+        y_mine = O.sj_apply(np.ascontiguousarray(mine), 0)
+        full = gather_shards(y_mine, first, job.shape[0])       # collection for checking only
+        if rank == 0:
+            q.put(("ok", bool(np.array_equal(full, O.sj_apply(job, 0))), int(mine.shape[0])))
+        else:
+            q.put(("ok", full is None, int(mine.shape[0])))
+    except Exception as e:  # pragma: no cover - reported to the parent
+        q.put(("error", repr(e), -1))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_transform_their_shards_and_stitch():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_transform_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    res = [q.get(timeout=10) for _ in range(2)]
+    assert all(r[0] == "ok" and r[1] is True for r in res), res
+    assert sorted(r[2] for r in res) == [18, 19]
+
+
+def test_apply_sharded_partition_logic_on_cpu():
+    """apply_sharded's split and stitch, with the oracle as each device's transform."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    x = np.random.default_rng(3).standard_normal((11, 8, 64)).astype(np.float32)
+    seen = []
+
+    def fake(piece, mode, dev):
+        seen.append((dev, piece.shape[0]))
+        return O.sj_apply(np.ascontiguousarray(piece), mode)
+
+    y = apply_sharded(x, 1, devices=[0, 1, 2], transform=fake)
+    assert seen == [(0, 4), (1, 4), (2, 3)]
+    assert np.array_equal(y, O.sj_apply(x, 1))
+    with pytest.raises(ValueError):
+        stitch([(0, x[:3]), (4, x[4:])], 11)
+    part, first = shard(x, 2, 3)
+    assert first == 8 and part.shape[0] == 3
