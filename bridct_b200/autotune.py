@@ -127,7 +127,8 @@ def tune_classes(items, x, tuning: Optional[Dict[str, int]] = None, steps: int =
     queue (a batch of that class's arrays only, at their own offsets), as its own fixed-shape
     launch, and for two-pass shapes with the few-array geometry; the fastest wins.  The chosen
     schedule is then timed on the whole batch for each side-stream count, next to the all-queue
-    and all-launch schedules, and the fastest whole-batch schedule is returned (its output checked
+    and all-launch schedules and a hybrid (whole-array classes in the queue, two-pass classes in
+    their own launches), and the fastest whole-batch schedule is returned (its output checked
     against the all-queue result).  Returns {"schedule", "ms", "queue_ms", "launch_ms", "classes"}."""
     import torch
 
@@ -150,8 +151,12 @@ def tune_classes(items, x, tuning: Optional[Dict[str, int]] = None, steps: int =
         del alone
     chosen = {r["class"]: r["choice"] for r in rows}
     every_launch = {r["class"]: min((k for k in r["ms"] if k != "queue"), key=r["ms"].get) for r in rows}
+    # Timed alone, a class of a few small arrays is all launch latency whatever its schedule; run
+    # together, the whole-array (tile) classes share one persistent launch beside the two-pass
+    # classes' own launches.
+    hybrid = {r["class"]: ("queue" if "launch_small" not in r["ms"] else every_launch[r["class"]]) for r in rows}
     trials = []
-    for name, classes in (("per_class", chosen), ("all_launch", every_launch)):
+    for name, classes in (("per_class", chosen), ("all_launch", every_launch), ("hybrid", hybrid)):
         for n in streams:
             trials.append((name, {"classes": classes, "streams": int(n)}))
     results = [("all_queue", {"classes": {}, "streams": 1}, _time_graph(lambda s: batch.apply(x, y, stream=s), x, steps))]

@@ -62,7 +62,8 @@ double sj_scale(int n, int k) {
 //   scale = s(G, d)          columns 1..15 when G < 32 (SJ scaled complex FFT),
 //           s(16, d >> 1)    columns 1..15 when G = 32 (split into two radix-2 halves),
 //           1                columns 0 and 16 (cooperative shuffle DFT across the lanes).
-// Fills caller-provided arrays of G*17 float2 (tw[b*17+c]) and G*17 float4 (post[d*17+c]).
+// Fills caller-provided arrays of G*17 float2 (tw[b*17+c]) and G*17 float4 (post at
+// post_index(G, d, c)).
 void fill_fourstep_tables(int N, float2* tw, float4* post) {
   const int G = N / 32;
   for (int b = 0; b < G; ++b)
@@ -82,7 +83,7 @@ void fill_fourstep_tables(int N, float2* tw, float4* post) {
       p.y = (float)(sig(k) * sg * std::sin(th));
       p.z = k ? (float)(sig(N - k) * sg * std::sin(th)) : 0.f;
       p.w = k ? (float)(-sig(N - k) * sg * std::cos(th)) : 0.f;
-      post[(size_t)d * 17 + c] = p;
+      post[post_index(G, d, c)] = p;
     }
 }
 
@@ -329,7 +330,7 @@ BRIDCT_API int bridct_plan_apply(bridct_plan* plan, enum bridct_mode mode, const
     if (pin_in) {
       e = cudaMemcpyAsync(plan->d_x, input, bytes, cudaMemcpyHostToDevice, st);
     } else {
-      memcpy(plan->pin, input, bytes);
+      host_copy(plan->pin, input, bytes);
       e = cudaMemcpyAsync(plan->d_x, plan->pin, bytes, cudaMemcpyHostToDevice, st);
     }
     if (e != cudaSuccess) return cuda_fail(e, "H2D");
@@ -351,7 +352,7 @@ BRIDCT_API int bridct_plan_apply(bridct_plan* plan, enum bridct_mode mode, const
   }
   e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_fail(e, "bridct_plan_apply");
-  if (!dy && !pin_out) memcpy(output, plan->pin + plan->elements, bytes);
+  if (!dy && !pin_out) host_copy(output, plan->pin + plan->elements, bytes);
   return BRIDCT_OK;
 }
 

@@ -99,6 +99,8 @@ int launch_plain_layout(DeviceCtx* d, int h, int w, int mode, const float* x, fl
 int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, size_t batch,
                         const float* dx, float* dy, bool pin_in, bool pin_out);
 bridct_plan* thread_square_plan(int n);
+// memcpy split over the library's host copy threads (pageable <-> pinned staging).
+void host_copy(void* dst, const void* src, size_t n);
 void release_plan_extras(bridct_plan* p);
 }  // namespace bridct
 

@@ -104,7 +104,7 @@ class CopyPool {
   std::deque<Job> jobs_;
 };
 
-static void host_copy(void* dst, const void* src, size_t n) { CopyPool::get().copy(dst, src, n); }
+void host_copy(void* dst, const void* src, size_t n) { CopyPool::get().copy(dst, src, n); }
 
 static constexpr size_t kChunkBytes = 8u << 20;      // staging per slot and direction
 static constexpr size_t kMinChunkBytes = 4u << 20;   // smallest chunk a call cuts

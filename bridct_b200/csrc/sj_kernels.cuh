@@ -290,7 +290,8 @@ __device__ __forceinline__ void tile_store(float* g, long long gp, int rows, int
 // Runs all lines of length N in a set of `nlines` lines; line l starts at tile + off(l),
 // elements at stride es.  Register lines (one thread per line) for N <= REG_MAX, warp
 // four-step lines above.
-template <int N, int MODE, int REG_MAX = 64, typename Off>
+// PAIRS: rows (es = 1) at 8-byte aligned starts; the four-step moves them in 64-bit pairs.
+template <int N, int MODE, int REG_MAX = 64, bool PAIRS = false, typename Off>
 __device__ __forceinline__ void run_lines(float* tile, int nlines, int es, const Off& off,
                                           float* xbuf, FourStepTables tab) {
   if constexpr (N <= REG_MAX) {
@@ -302,7 +303,7 @@ __device__ __forceinline__ void run_lines(float* tile, int nlines, int es, const
     float* xb = xbuf + warp * FourStepSizes<G>::FLOATS;
     for (int g = warp; g * LPW < nlines; g += blockDim.x >> 5) {
       auto ptr = [&](int j) { return tile + off(g * LPW + j); };
-      fs_line<G, MODE>(ptr, es, xb, tab);
+      fs_line<G, MODE, PAIRS>(ptr, es, xb, tab);
     }
   }
 }
@@ -369,7 +370,8 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
       __syncthreads();
     }
     if constexpr (DO_ROW) {
-      run_lines<W, MODE, reg_line_max(W, H, MODE, !DO_COL)>(tile, TR, 1, [](int l) { return l * P; }, xbuf, trow);
+      run_lines<W, MODE, reg_line_max(W, H, MODE, !DO_COL), P % 2 == 0>(tile, TR, 1, [](int l) { return l * P; },
+                                                                         xbuf, trow);
       __syncthreads();
     }
     if constexpr (GEN) tile_store_rows<P>(yrow(t), rows, W, tile);

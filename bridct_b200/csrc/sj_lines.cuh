@@ -104,6 +104,14 @@ struct FourStepTables {
   const float4* post;
 };
 
+// Position of post coefficient (d, c) in the table of lines of N = 32 G points: [d][c] (17 per d)
+// for G < 32.  For G = 32 the table is [d / 2][c][d % 2]: the 30 stage-2 lanes of one step, lane
+// (c, h) reading d = 2 m + h, then read 30 consecutive float4s (a [d][c] table put lanes (c, 0) and
+// (c, 1) 17 float4s apart: 2-way bank conflicts on every read).  Host and device use this function.
+__host__ __device__ constexpr int post_index(int G, int d, int c) {
+  return G == 32 ? (d >> 1) * 34 + 2 * c + (d & 1) : d * 17 + c;
+}
+
 // Exchange buffer floats needed per warp for a given G (re and im planes).
 template <int G>
 struct FourStepSizes {
@@ -232,7 +240,12 @@ __device__ __forceinline__ void post_load(const float* line, int es, int N, int 
 //             pre-rotated by w_N^{16 b}); lane b stores V(bitrev(b)) where that index is needed
 //   stage 2   columns 1..15: generated SJ complex FFT of length G per task (G = 32: each column
 //             split into its two radix-2 halves, so 30 lanes do equal work)
-template <int G, typename LinePtr>
+// PAIRS: the lines are rows (es = 1) starting 8-byte aligned.  Makhoul's v[n] = x[2n] and
+// v[N-1-n] = x[2n+1] (n < N/2) then come from one 64-bit load: lane b keeps x[2n] (n = G a + b,
+// a < 16) and passes x[2n+1] = v[N-1-n] = v[G (31 - a) + (G-1-b)] to lane G-1-b, whose element
+// 31 - a it is.  Half the load instructions, and no 2-way bank conflict of the stride-2 scalar
+// gather.
+template <int G, bool PAIRS = false, typename LinePtr>
 __device__ __forceinline__ void fs_forward(const LinePtr& line_ptr, int es, float* xb,
                                            FourStepTables tab) {
   constexpr int N = 32 * G;
@@ -243,8 +256,17 @@ __device__ __forceinline__ void fs_forward(const LinePtr& line_ptr, int es, floa
   {
     float* line = line_ptr(grp);
     float xin[32], w[32];
+    if constexpr (PAIRS) {
 #pragma unroll
-    for (int a = 0; a < 32; ++a) xin[a] = line[makhoul_src(G * a + b, N) * es];
+      for (int a = 0; a < 16; ++a) {
+        const float2 p = *reinterpret_cast<const float2*>(line + 2 * (G * a + b));
+        xin[a] = p.x;
+        xin[31 - a] = __shfl_xor_sync(0xFFFFFFFFu, p.y, G - 1);
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < 32; ++a) xin[a] = line[makhoul_src(G * a + b, N) * es];
+    }
     sj_rfft_32(xin, w);
     float* re = xb + fs_slot<G>(grp, es == 1) * SZ::LINE + b;
     float* im = re + SZ::PLANE;
@@ -268,8 +290,8 @@ __device__ __forceinline__ void fs_forward(const LinePtr& line_ptr, int es, floa
   {
     float* line = line_ptr(grp);
     const int d = bitrev<G>(b);
-    if (d <= G / 2) post_store(line, es, N, 32 * d, tab.post[d * 17], ar, (d == 0 || d == G / 2) ? 0.0f : ai);
-    if (d < G / 2) post_store(line, es, N, 16 + 32 * d, tab.post[d * 17 + 16], cr, ci);
+    if (d <= G / 2) post_store(line, es, N, 32 * d, tab.post[post_index(G, d, 0)], ar, (d == 0 || d == G / 2) ? 0.0f : ai);
+    if (d < G / 2) post_store(line, es, N, 16 + 32 * d, tab.post[post_index(G, d, 16)], cr, ci);
   }
   if constexpr (G == 32) {
     if (lane < 30) {
@@ -285,10 +307,17 @@ __device__ __forceinline__ void fs_forward(const LinePtr& line_ptr, int es, floa
       }
       if (h) sj_cfft_32_half1(z, o);
       else sj_cfft_32_half0(z, o);
+      // Lanes (c, 0) and (c, 1) would store y[k] and y[k + 32] (one bank) at once: lane h = 1
+      // stores its y[N - k] first instead (bank -k, disjoint from the h = 0 lanes' banks k, for
+      // rows and for the odd pitches of 512/1024-point column strips alike).
 #pragma unroll
       for (int m = 0; m < 16; ++m) {
-        const int dd = 2 * m + h;
-        post_store(line, es, N, c + 32 * dd, tab.post[dd * 17 + c], o[2 * m], o[2 * m + 1]);
+        const int dd = 2 * m + h, k = c + 32 * dd;
+        const float4 pc = tab.post[post_index(G, dd, c)];
+        const float vr = o[2 * m], vi = o[2 * m + 1];
+        const float yk = pc.x * vr + pc.y * vi, ynk = pc.z * vr + pc.w * vi;
+        line[(h ? N - k : k) * es] = h ? ynk : yk;
+        line[(h ? k : N - k) * es] = h ? yk : ynk;
       }
     }
   } else {
@@ -307,14 +336,16 @@ __device__ __forceinline__ void fs_forward(const LinePtr& line_ptr, int es, floa
       }
       CFFT<G>::fwd(z);
 #pragma unroll
-      for (int dd = 0; dd < G; ++dd) post_store(line, es, N, c + 32 * dd, tab.post[dd * 17 + c], z[2 * dd], z[2 * dd + 1]);
+      for (int dd = 0; dd < G; ++dd)
+        post_store(line, es, N, c + 32 * dd, tab.post[post_index(G, dd, c)], z[2 * dd], z[2 * dd + 1]);
     }
   }
   __syncwarp();
 }
 
-// Transpose of fs_forward: orthonormal DCT-III on the warp's lines.
-template <int G, typename LinePtr>
+// Transpose of fs_forward: orthonormal DCT-III on the warp's lines (PAIRS: 64-bit stores of
+// x[2n], x[2n+1], the odd element taken from lane G-1-b).
+template <int G, bool PAIRS = false, typename LinePtr>
 __device__ __forceinline__ void fs_inverse(const LinePtr& line_ptr, int es, float* xb,
                                            FourStepTables tab) {
   constexpr int N = 32 * G;
@@ -327,10 +358,10 @@ __device__ __forceinline__ void fs_inverse(const LinePtr& line_ptr, int es, floa
     const float* line = line_ptr(grp);
     const int d = bitrev<G>(b);
     if (d <= G / 2) {
-      post_load(line, es, N, 32 * d, tab.post[d * 17], ar, ai);
+      post_load(line, es, N, 32 * d, tab.post[post_index(G, d, 0)], ar, ai);
       if (d == 0 || d == G / 2) ai = 0.0f;
     }
-    if (d < G / 2) post_load(line, es, N, 16 + 32 * d, tab.post[d * 17 + 16], cr, ci);
+    if (d < G / 2) post_load(line, es, N, 16 + 32 * d, tab.post[post_index(G, d, 16)], cr, ci);
   }
   coop_dft_t<G>(ar, ai, b, tab.tw);
   coop_dft_t<G>(cr, ci, b, tab.tw);
@@ -345,9 +376,17 @@ __device__ __forceinline__ void fs_inverse(const LinePtr& line_ptr, int es, floa
       const int c = 1 + (lane >> 1), h = lane & 1;
       float o[32], z[64];
 #pragma unroll
-      for (int m = 0; m < 16; ++m) {
-        const int dd = 2 * m + h;
-        post_load(line, es, N, c + 32 * dd, tab.post[dd * 17 + c], o[2 * m], o[2 * m + 1]);
+      for (int m = 0; m < 16; ++m) {       // loads in the bank-disjoint order of the forward's stores
+        const int dd = 2 * m + h, k = c + 32 * dd;
+        const float4 pc = tab.post[post_index(G, dd, c)];
+        const float first = line[(h ? N - k : k) * es];
+        const float second = line[(h ? k : N - k) * es];
+        const float yk = h ? second : first, ynk = h ? first : second;
+        float vr = pc.x * yk, vi = pc.y * yk;   // the arithmetic of post_load
+        vr += pc.z * ynk;
+        vi += pc.w * ynk;
+        o[2 * m] = vr;
+        o[2 * m + 1] = vi;
       }
       if (h) sj_cfft_32_half1_t(o, z);
       else sj_cfft_32_half0_t(o, z);
@@ -371,7 +410,8 @@ __device__ __forceinline__ void fs_inverse(const LinePtr& line_ptr, int es, floa
       float* im = re + SZ::PLANE;
       float z[2 * G];
 #pragma unroll
-      for (int dd = 0; dd < G; ++dd) post_load(line, es, N, c + 32 * dd, tab.post[dd * 17 + c], z[2 * dd], z[2 * dd + 1]);
+      for (int dd = 0; dd < G; ++dd)
+        post_load(line, es, N, c + 32 * dd, tab.post[post_index(G, dd, c)], z[2 * dd], z[2 * dd + 1]);
       CFFT<G>::tr(z);
 #pragma unroll
       for (int q = 0; q < G; ++q) {
@@ -396,22 +436,30 @@ __device__ __forceinline__ void fs_inverse(const LinePtr& line_ptr, int es, floa
     w[16] = w16;
     sj_rfft_32_t(w, xo);
     float* line = line_ptr(grp);
+    if constexpr (PAIRS) {
 #pragma unroll
-    for (int a = 0; a < 32; ++a) line[makhoul_src(G * a + b, N) * es] = xo[a];
+      for (int a = 0; a < 16; ++a) {
+        const float odd = __shfl_xor_sync(0xFFFFFFFFu, xo[31 - a], G - 1);
+        *reinterpret_cast<float2*>(line + 2 * (G * a + b)) = make_float2(xo[a], odd);
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < 32; ++a) line[makhoul_src(G * a + b, N) * es] = xo[a];
+    }
   }
   __syncwarp();
 }
 
-template <int G, int MODE, typename LinePtr>
+template <int G, int MODE, bool PAIRS = false, typename LinePtr>
 __device__ __forceinline__ void fs_line(const LinePtr& line_ptr, int es, float* xb,
                                         FourStepTables tab) {
   if (MODE == LM_FWD) {
-    fs_forward<G>(line_ptr, es, xb, tab);
+    fs_forward<G, PAIRS>(line_ptr, es, xb, tab);
   } else if (MODE == LM_INV) {
-    fs_inverse<G>(line_ptr, es, xb, tab);
+    fs_inverse<G, PAIRS>(line_ptr, es, xb, tab);
   } else {
-    fs_forward<G>(line_ptr, es, xb, tab);
-    fs_inverse<G>(line_ptr, es, xb, tab);
+    fs_forward<G, PAIRS>(line_ptr, es, xb, tab);
+    fs_inverse<G, PAIRS>(line_ptr, es, xb, tab);
   }
 }
 

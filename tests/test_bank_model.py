@@ -113,3 +113,54 @@ def test_odd_pitch_of_1024_point_strips():
     for tc in (8, 16):
         odd, even = four_step_wavefronts(32, tc + 1, rows=False), four_step_wavefronts(32, tc + 2, rows=False)
         assert even > 1.2 * odd
+
+
+def g32_post_store_wavefronts(es, swapped):
+    """Stage-2 post-rotation stores of a 1024-point line (G = 32): lane l < 30 owns column
+    c = 1 + l // 2 and the half h = l % 2 (d = 2 m + h); at step m it stores y[k] and y[N - k],
+    k = c + 32 d.  swapped: lanes with h = 1 store y[N - k] first (fs_forward)."""
+    n, total = 1024, 0
+    for m in range(16):
+        first, second = [], []
+        for l in range(32):
+            if l >= 30:
+                first.append(None)
+                second.append(None)
+                continue
+            c, h = 1 + l // 2, l % 2
+            k = c + 32 * (2 * m + h)
+            a, b = (n - k, k) if (swapped and h) else (k, n - k)
+            first.append(a * es)
+            second.append(b * es)
+        total += wavefronts(first) + wavefronts(second)
+    return total
+
+
+def test_g32_post_stores_are_bank_disjoint_after_the_swap():
+    # rows (es = 1) and the odd pitches of 1024-point column strips (tc + 1 = 9, 17)
+    for es in (1, 9, 17):
+        assert g32_post_store_wavefronts(es, swapped=True) == 32          # one wavefront per store
+        assert g32_post_store_wavefronts(es, swapped=False) == 64         # lanes (c, 0), (c, 1) collide
+
+
+def test_paired_row_gather_has_no_conflicts():
+    """Row lines read Makhoul's v[n] = x[2n], v[N-1-n] = x[2n+1] as 64-bit pairs: one 64-bit access
+    per lane (two wavefronts for 32 lanes, the minimum) instead of two scalar stride-2 accesses of
+    two wavefronts each."""
+    for g, pitch in ((4, 128 + 4), (8, 256 + 8), (16, 512 + 16), (32, 1024 + 4)):   # the row-block pitches
+        n = 32 * g
+        pair_words = []
+        for a in range(16):
+            words = []
+            for l in range(32):
+                j, b = l // g, l % g
+                words += [j * pitch + 2 * (g * a + b), j * pitch + 2 * (g * a + b) + 1]
+            # a 64-bit warp access is serviced per half warp
+            pair_words.append(wavefronts(words[:32]) + wavefronts(words[32:]))
+        scalar = [wavefronts([(l // g) * pitch + makhoul_src(g * a + l % g, n) for l in range(32)])
+                  for a in range(32)]
+        # half the instructions always; conflict-free from 256-point rows on (128-point rows, eight
+        # to a warp at pitch 132, keep the scalar gather's count)
+        assert sum(pair_words) <= sum(scalar), g
+        if g >= 8:
+            assert sum(pair_words) == 32 and sum(scalar) == 64, (g, sum(pair_words), sum(scalar))
