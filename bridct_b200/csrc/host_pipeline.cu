@@ -62,7 +62,9 @@ class CopyPool {
   }
 
  private:
-  static constexpr size_t kPiece = 1u << 20;   // copies below 2 MB stay on the calling thread
+  // Pieces of at least 256 KB: an 8 MB slot is split over every thread (one thread's memcpy into
+  // pinned memory measured 16.6 GB/s on a B200 host, twelve threads together 67 GB/s).
+  static constexpr size_t kPiece = 256u << 10;
   struct Call {
     std::mutex mu;
     std::condition_variable cv;

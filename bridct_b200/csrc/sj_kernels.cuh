@@ -370,8 +370,11 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
       __syncthreads();
     }
     if constexpr (DO_ROW) {
-      run_lines<W, MODE, reg_line_max(W, H, MODE, !DO_COL), P % 2 == 0>(tile, TR, 1, [](int l) { return l * P; },
-                                                                         xbuf, trow);
+      // Paired 64-bit gathers for 512- and 1024-point rows only: they remove the stride-2 bank
+      // conflicts there, while 256-point rows (no fewer wavefronts at their pitch, plus the
+      // shuffles) measured 7-12% slower with them.
+      run_lines<W, MODE, reg_line_max(W, H, MODE, !DO_COL), P % 2 == 0 && W >= 512>(
+          tile, TR, 1, [](int l) { return l * P; }, xbuf, trow);
       __syncthreads();
     }
     if constexpr (GEN) tile_store_rows<P>(yrow(t), rows, W, tile);
