@@ -26,9 +26,17 @@ static int kernel_blocks_per_sm(Kernel k, int smem, int threads = kThreads) {
 // CTAs may be scheduled, and run up to their first global access, while the previous kernel in
 // the stream finishes, which hides most of the launch gap between back-to-back launches (the two
 // passes of a two-pass shape, or consecutive calls).
+// With pdl = false it is an ordinary launch (the kernels' griddepcontrol instructions are then
+// no-ops).  Measured on 128 MiB batches of every shape (two A/B runs on one box): +1..5% on every
+// single-kernel shape, but 6..10% slower on most two-pass shapes with full-grid passes (the passes
+// of the few-array geometry keep it: one 1024 x 1024 array 529 -> 577 GB/s).
 template <typename... Params, typename... Args>
 static cudaError_t launch_pdl(void (*k)(Params...), unsigned grid, unsigned threads, int smem, cudaStream_t st,
-                              Args... args) {
+                              bool pdl, Args... args) {
+  if (!pdl) {
+    k<<<grid, threads, smem, st>>>(args...);
+    return cudaGetLastError();
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(threads);
@@ -44,12 +52,12 @@ static cudaError_t launch_pdl(void (*k)(Params...), unsigned grid, unsigned thre
 
 template <typename Kernel>
 static cudaError_t launch_tiles(Kernel k, int smem, int bps, TileArgs a, const LaunchCtx& ctx,
-                                cudaStream_t st, int threads = kThreads) {
+                                cudaStream_t st, int threads = kThreads, bool pdl = true) {
   if (bps <= 0) return cudaErrorInvalidConfiguration;
   if (a.ntiles <= 0) return cudaSuccess;
   long long grid = (long long)ctx.sm_count * bps;
   if (grid > a.ntiles) grid = a.ntiles;
-  return launch_pdl(k, (unsigned)grid, (unsigned)threads, smem, st, a);
+  return launch_pdl(k, (unsigned)grid, (unsigned)threads, smem, st, pdl, a);
 }
 
 // GEN: the batch has general layouts (strided arrays or an offset table, BatchLayout); the same
@@ -75,7 +83,7 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
       const long long ntiles = (batch + kB8dbThreads - 1) / kB8dbThreads;
       long long grid = (long long)ctx.sm_count * bps;
       if (grid > ntiles) grid = ntiles;
-      return launch_pdl(k, (unsigned)grid, kB8dbThreads, smem, st, x, y, batch);
+      return launch_pdl(k, (unsigned)grid, kB8dbThreads, smem, st, true, x, y, batch);
     }
     auto k = k_blocks8<MODE>;
     constexpr int smem = kB8Chunks * 16;
@@ -84,7 +92,7 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     const long long ntiles = (batch + kB8Threads - 1) / kB8Threads;
     long long grid = (long long)ctx.sm_count * bps;
     if (grid > ntiles) grid = ntiles;
-    return launch_pdl(k, (unsigned)grid, kB8Threads, smem, st, x, y, batch);
+    return launch_pdl(k, (unsigned)grid, kB8Threads, smem, st, true, x, y, batch);
   } else if constexpr (Gm::kTile) {
     // 16384-float tiles instead of 8192 where they measured faster on 128 MiB batches: 64-wide
     // arrays up to 64 high (+6..14%, except the 64 x 64 inverse, -2%) and forward/inverse of
@@ -130,23 +138,26 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     // 2048 x 256^2 1669 -> 2129 GB/s).
     const long long nb = batch;
     cudaError_t e;
-    const bool small = nb * (W / Gm::kTC) < 2LL * ctx.sm_count || (GEN && lx.small_units);
+    const bool few = nb * (W / Gm::kTC) < 2LL * ctx.sm_count;   // passes below a full grid: PDL
+    const bool small = few || (GEN && lx.small_units);
     if (small) {   // few arrays (or asked for): smaller strips and row blocks
       auto kcs = k_colstrip<H, W, Gm::kTCs, MODE, TC_T, GEN>;
       TileArgs ac{x, y, nb * (W / Gm::kTCs), nb * H, tab, lx, ly};
-      e = launch_tiles(kcs, Gm::kSmemStripS, kernel_blocks_per_sm(kcs, Gm::kSmemStripS, TC_T), ac, ctx, st, TC_T);
+      e = launch_tiles(kcs, Gm::kSmemStripS, kernel_blocks_per_sm(kcs, Gm::kSmemStripS, TC_T), ac, ctx, st, TC_T,
+                       few);
     } else {
       TileArgs ac{x, y, nb * (W / Gm::kTC), nb * H, tab, lx, ly};
-      e = launch_tiles(kc, Gm::kSmemStrip, bpc, ac, ctx, st, TC_T);
+      e = launch_tiles(kc, Gm::kSmemStrip, bpc, ac, ctx, st, TC_T, false);
     }
     if (e != cudaSuccess) return e;
     if (nb * H / Gm::kRB < 2LL * ctx.sm_count || (GEN && lx.small_units)) {
       auto krs = k_full<H, W, Gm::kRBs, false, true, MODE, TR_T, GEN>;
       TileArgs ar{y, y, nb * H / Gm::kRBs, nb * H, tab, ly, ly};
-      e = launch_tiles(krs, Gm::kSmemRowsS, kernel_blocks_per_sm(krs, Gm::kSmemRowsS, TR_T), ar, ctx, st, TR_T);
+      e = launch_tiles(krs, Gm::kSmemRowsS, kernel_blocks_per_sm(krs, Gm::kSmemRowsS, TR_T), ar, ctx, st, TR_T,
+                       few);
     } else {
       TileArgs ar{y, y, nb * H / Gm::kRB, nb * H, tab, ly, ly};
-      e = launch_tiles(kr, Gm::kSmemRows, bpr, ar, ctx, st, TR_T);
+      e = launch_tiles(kr, Gm::kSmemRows, bpr, ar, ctx, st, TR_T, false);
     }
     if (e != cudaSuccess) return e;
     return cudaSuccess;
