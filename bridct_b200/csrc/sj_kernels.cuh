@@ -385,13 +385,24 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
 
 // Column strips: H rows x TC columns of one array (row pitch W in global memory; ld of the
 // layouts with GEN).
+// 1024-high strips are staged transposed: column c of the strip is row c of the tile (pitch
+// transposed_pitch), so the column lines run the row-line code (64-bit paired Makhoul gathers,
+// bank-disjoint post stores) instead of a stride-pitch walk down the tile, whose stride-2 Makhoul
+// gather is 2-way bank-conflicted at any pitch.  The transposing scalar stores of the staging are
+// conflict-free at this pitch: a warp covers 32 / (TC / 4) rows of TC / 4 float4 groups, and group
+// q's stores land 4 q * pitch = q * 128 / TC (mod 32) banks apart.
+template <int H> __host__ __device__ constexpr bool transposed_strip() { return H == 1024; }
+__host__ __device__ constexpr int transposed_pitch(int h, int tc) { return h + (tc >= 8 ? 32 / tc : 4); }
+
 template <int H, int W, int TC, int MODE, int THREADS = kThreads, bool GEN = false>
 __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
-  constexpr int P = strip_pitch(H, TC);
+  constexpr bool kT = transposed_strip<H>();
+  static_assert(!kT || TC <= 8, "transposed strips hold at most 8 columns");
+  constexpr int P = kT ? transposed_pitch(H, TC) : strip_pitch(H, TC);
   constexpr int STRIPS = W / TC;
   extern __shared__ float smem[];
   float* tile = smem;
-  float* xbuf = smem + round4(H * P);
+  float* xbuf = smem + round4(kT ? TC * P : H * P);
   griddep_wait();
   const FourStepTables tcol = stage_tables<H>(a.tab.col, xbuf + round4((THREADS / 32) * ExchangeFloats<H>::value));
   // Strips of 128- and 256-point columns prefetch the next strip into registers during the
@@ -411,13 +422,39 @@ __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
       next.put(tile);
       __syncthreads();
       if (t + gridDim.x < a.ntiles) next.load(src(t + gridDim.x), xp, H);
+    } else if constexpr (kT) {
+      const float* g = xarr(arr) + s * TC;
+      constexpr int Q = TC / 4;
+      for (int i = threadIdx.x; i < H * Q; i += THREADS) {
+        const int r = i / Q, c = (i % Q) * 4;
+        const float4 v = __ldg(reinterpret_cast<const float4*>(g + r * xp + c));
+        tile[c * P + r] = v.x;
+        tile[(c + 1) * P + r] = v.y;
+        tile[(c + 2) * P + r] = v.z;
+        tile[(c + 3) * P + r] = v.w;
+      }
+      __syncthreads();
     } else {
       tile_load<P>(xarr(arr) + s * TC, xp, H, TC, tile, H);
       __syncthreads();
     }
-    run_lines<H, MODE, reg_line_max(H, W, MODE, true)>(tile, TC, P, [](int l) { return l; }, xbuf, tcol);
+    if constexpr (kT) {
+      run_lines<H, MODE, reg_line_max(H, W, MODE, true), true>(tile, TC, 1, [](int l) { return l * P; }, xbuf, tcol);
+    } else {
+      run_lines<H, MODE, reg_line_max(H, W, MODE, true)>(tile, TC, P, [](int l) { return l; }, xbuf, tcol);
+    }
     __syncthreads();
-    tile_store<P>(yarr(arr) + s * TC, yp, H, TC, tile);
+    if constexpr (kT) {
+      float* g = yarr(arr) + s * TC;
+      constexpr int Q = TC / 4;
+      for (int i = threadIdx.x; i < H * Q; i += THREADS) {
+        const int r = i / Q, c = (i % Q) * 4;
+        *reinterpret_cast<float4*>(g + r * yp + c) =
+            make_float4(tile[c * P + r], tile[(c + 1) * P + r], tile[(c + 2) * P + r], tile[(c + 3) * P + r]);
+      }
+    } else {
+      tile_store<P>(yarr(arr) + s * TC, yp, H, TC, tile);
+    }
     __syncthreads();
   }
 }
@@ -454,8 +491,11 @@ struct Geometry {
   // the two-pass shapes and modes where it measured faster than the two passes (launch_plain).
   static constexpr int kSmemWhole = full_smem(1);
   // 2-pass class
+  static constexpr int strip_tile(int tc) {
+    return transposed_strip<H>() ? tc * transposed_pitch(H, tc) : H * strip_pitch(H, tc);
+  }
   static constexpr int strip_smem(int tc) {
-    return (round4(H * strip_pitch(H, tc)) + round4(kWarps * ExchangeFloats<H>::value) + TableFloats<H>::value) * 4;
+    return (round4(strip_tile(tc)) + round4(kWarps * ExchangeFloats<H>::value) + TableFloats<H>::value) * 4;
   }
   // The strip width is sized with pitch tc + 4 even where the strip uses tc + 2: 256-point strips
   // widened to 64 columns by the smaller pitch measured 4-11% slower.
