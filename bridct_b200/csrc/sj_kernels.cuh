@@ -385,19 +385,23 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
 
 // Column strips: H rows x TC columns of one array (row pitch W in global memory; ld of the
 // layouts with GEN).
-// 1024-high strips are staged transposed: column c of the strip is row c of the tile (pitch
-// transposed_pitch), so the column lines run the row-line code (64-bit paired Makhoul gathers,
-// bank-disjoint post stores) instead of a stride-pitch walk down the tile, whose stride-2 Makhoul
-// gather is 2-way bank-conflicted at any pitch.  The transposing scalar stores of the staging are
-// conflict-free at this pitch: a warp covers 32 / (TC / 4) rows of TC / 4 float4 groups, and group
-// q's stores land 4 q * pitch = q * 128 / TC (mod 32) banks apart.
-template <int H> __host__ __device__ constexpr bool transposed_strip() { return H == 1024; }
-__host__ __device__ constexpr int transposed_pitch(int h, int tc) { return h + (tc >= 8 ? 32 / tc : 4); }
+// Strips of 1024-point columns (8 wide) and 512-point columns (32 wide) are staged transposed:
+// column c of the strip is row c of the tile (pitch transposed_pitch), so the column lines run the
+// row-line code instead of a stride-pitch walk down the tile, whose stride-2 Makhoul gather is
+// 2-way bank-conflicted at any pitch.  1024: pitch 1028, the row blocks' pitch, with 64-bit paired
+// gathers.  512: pitch 529 (= 17 mod 32); the bank model (tests/test_bank_model.py) counts 158
+// wavefronts per warp for 512-point rows at that pitch against 190 for the 34-pitch column walk,
+// and the scalar gathers of a warp's two lines fall into even and odd banks.  The transposing
+// scalar stores of the staging are conflict-free at both pitches: a warp covers 32 / (TC / 4) rows
+// of TC / 4 float4 groups, and group q's stores land 4 q * pitch = q * 128 / TC (mod 32) banks apart.
+template <int H, int TC> __host__ __device__ constexpr bool transposed_strip() {
+  return (H == 1024 && TC == 8) || (H == 512 && TC == 32);
+}
+__host__ __device__ constexpr int transposed_pitch(int h, int tc) { return h == 1024 ? 1028 : tc == 32 ? h + 17 : h + 4; }
 
 template <int H, int W, int TC, int MODE, int THREADS = kThreads, bool GEN = false>
 __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
-  constexpr bool kT = transposed_strip<H>();
-  static_assert(!kT || TC <= 8, "transposed strips hold at most 8 columns");
+  constexpr bool kT = transposed_strip<H, TC>();
   constexpr int P = kT ? transposed_pitch(H, TC) : strip_pitch(H, TC);
   constexpr int STRIPS = W / TC;
   extern __shared__ float smem[];
@@ -423,15 +427,26 @@ __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
       __syncthreads();
       if (t + gridDim.x < a.ntiles) next.load(src(t + gridDim.x), xp, H);
     } else if constexpr (kT) {
+      // eight float4 loads in flight per thread before their transposing stores
       const float* g = xarr(arr) + s * TC;
-      constexpr int Q = TC / 4;
-      for (int i = threadIdx.x; i < H * Q; i += THREADS) {
-        const int r = i / Q, c = (i % Q) * 4;
-        const float4 v = __ldg(reinterpret_cast<const float4*>(g + r * xp + c));
-        tile[c * P + r] = v.x;
-        tile[(c + 1) * P + r] = v.y;
-        tile[(c + 2) * P + r] = v.z;
-        tile[(c + 3) * P + r] = v.w;
+      constexpr int Q = TC / 4, kPer = H * Q / THREADS, kBatch = kPer < 8 ? kPer : 8;
+      static_assert(kPer % kBatch == 0, "strip staging batches");
+#pragma unroll 1
+      for (int k0 = 0; k0 < kPer; k0 += kBatch) {
+        float4 v[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+          const int i = threadIdx.x + (k0 + k) * THREADS, r = i / Q, c = (i % Q) * 4;
+          v[k] = __ldg(reinterpret_cast<const float4*>(g + r * xp + c));
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+          const int i = threadIdx.x + (k0 + k) * THREADS, r = i / Q, c = (i % Q) * 4;
+          tile[c * P + r] = v[k].x;
+          tile[(c + 1) * P + r] = v[k].y;
+          tile[(c + 2) * P + r] = v[k].z;
+          tile[(c + 3) * P + r] = v[k].w;
+        }
       }
       __syncthreads();
     } else {
@@ -439,7 +454,8 @@ __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
       __syncthreads();
     }
     if constexpr (kT) {
-      run_lines<H, MODE, reg_line_max(H, W, MODE, true), true>(tile, TC, 1, [](int l) { return l * P; }, xbuf, tcol);
+      run_lines<H, MODE, reg_line_max(H, W, MODE, true), P % 2 == 0>(tile, TC, 1, [](int l) { return l * P; },
+                                                                    xbuf, tcol);
     } else {
       run_lines<H, MODE, reg_line_max(H, W, MODE, true)>(tile, TC, P, [](int l) { return l; }, xbuf, tcol);
     }
@@ -492,7 +508,7 @@ struct Geometry {
   static constexpr int kSmemWhole = full_smem(1);
   // 2-pass class
   static constexpr int strip_tile(int tc) {
-    return transposed_strip<H>() ? tc * transposed_pitch(H, tc) : H * strip_pitch(H, tc);
+    return (H == 1024 && tc == 8) || (H == 512 && tc == 32) ? tc * transposed_pitch(H, tc) : H * strip_pitch(H, tc);
   }
   static constexpr int strip_smem(int tc) {
     return (round4(strip_tile(tc)) + round4(kWarps * ExchangeFloats<H>::value) + TableFloats<H>::value) * 4;

@@ -165,3 +165,14 @@ def test_paired_row_gather_has_no_conflicts():
         assert sum(pair_words) <= sum(scalar), g
         if g >= 16:
             assert sum(pair_words) == 32 and sum(scalar) == 64, (g, sum(pair_words), sum(scalar))
+
+
+def test_transposed_512_point_strips():
+    """512-point column strips (32 wide) are staged transposed at pitch 529: the column lines then
+    walk as rows, which the model counts cheaper than the 34-pitch column walk, and the transposing
+    scalar stores of the staging (a warp: 4 rows x 8 float4 groups) are conflict-free."""
+    assert four_step_wavefronts(16, 529, rows=True) < 0.9 * four_step_wavefronts(16, 34, rows=False)
+    for pitch, tc in ((529, 32), (1028, 8)):
+        q = tc // 4
+        for j in range(4):
+            assert wavefronts([(4 * (l % q) + j) * pitch + l // q for l in range(32)]) == 1
