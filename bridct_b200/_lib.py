@@ -12,7 +12,7 @@ FORWARD, INVERSE, ROUNDTRIP = 0, 1, 2
 OK, INVALID_ARGUMENT, WORKSPACE_TOO_SMALL, BAD_ALIGNMENT, OVERLAPPING_BUFFERS = 0, -1, -2, -3, -4
 DEVICE_ERROR, TIMEOUT = -5, -6
 FORM_SJ, FORM_TC_BF16X3, FORM_TC_TF32X3, FORM_TC_FP8 = 0, 1, 2, 3
-RAGGED_QUEUE, RAGGED_CLASS_LAUNCH, RAGGED_CLASS_LAUNCH_SMALL = 0, 1, 2
+RAGGED_QUEUE, RAGGED_CLASS_LAUNCH, RAGGED_CLASS_LAUNCH_SMALL, RAGGED_MERGED = 0, 1, 2, 3
 VERSION = "0.2.0-dev.7"
 
 _FP = C.POINTER(C.c_float)

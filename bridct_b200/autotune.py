@@ -127,9 +127,10 @@ def tune_classes(items, x, tuning: Optional[Dict[str, int]] = None, steps: int =
     queue (a batch of that class's arrays only, at their own offsets), as its own fixed-shape
     launch, and for two-pass shapes with the few-array geometry; the fastest wins.  The chosen
     schedule is then timed on the whole batch for each side-stream count, next to the all-queue
-    and all-launch schedules and a hybrid (whole-array classes in the queue, two-pass classes in
-    their own launches), and the fastest whole-batch schedule is returned (its output checked
-    against the all-queue result).  Returns {"schedule", "ms", "queue_ms", "launch_ms", "classes"}."""
+    and all-launch schedules, a hybrid (whole-array classes in the queue, two-pass classes in
+    their own launches) and a merged schedule (two-pass classes in merged column and row passes),
+    and the fastest whole-batch schedule is returned (its output checked against the all-queue
+    result).  Returns {"schedule", "ms", "queue_ms", "launch_ms", "classes"}."""
     import torch
 
     from .ragged import RaggedBatch
@@ -155,8 +156,21 @@ def tune_classes(items, x, tuning: Optional[Dict[str, int]] = None, steps: int =
     # together, the whole-array (tile) classes share one persistent launch beside the two-pass
     # classes' own launches.
     hybrid = {r["class"]: ("queue" if "launch_small" not in r["ms"] else every_launch[r["class"]]) for r in rows}
+    # merged: the two-pass classes share one column-pass launch per column length and mode and one
+    # row-pass launch per row length and mode (far fewer launches and tails); whole 32768-float
+    # arrays keep their own launch, the rest the queue
+    from .ragged import two_pass
+
+    def merged_choice(r):
+        h, w, m = (int(v) for v in r["class"].replace("/", "x").split("x"))
+        if two_pass(h, w, m):
+            return "merged"
+        return "queue" if "launch_small" not in r["ms"] else every_launch[r["class"]]
+
+    merged = {r["class"]: merged_choice(r) for r in rows}
     trials = []
-    for name, classes in (("per_class", chosen), ("all_launch", every_launch), ("hybrid", hybrid)):
+    for name, classes in (("per_class", chosen), ("all_launch", every_launch), ("hybrid", hybrid),
+                          ("merged", merged)):
         for n in streams:
             trials.append((name, {"classes": classes, "streams": int(n)}))
     results = [("all_queue", {"classes": {}, "streams": 1}, _time_graph(lambda s: batch.apply(x, y, stream=s), x, steps))]

@@ -94,14 +94,43 @@ void build_fourstep_tables(int N, std::vector<float2>& tw, std::vector<float4>& 
   fill_fourstep_tables(N, tw.data(), post.data());
 }
 
-void plain_table_h8(PlainLauncher (*row)[3]);
-void plain_table_h16(PlainLauncher (*row)[3]);
-void plain_table_h32(PlainLauncher (*row)[3]);
-void plain_table_h64(PlainLauncher (*row)[3]);
-void plain_table_h128(PlainLauncher (*row)[3]);
-void plain_table_h256(PlainLauncher (*row)[3]);
-void plain_table_h512(PlainLauncher (*row)[3]);
-void plain_table_h1024(PlainLauncher (*row)[3]);
+#define BRIDCT_DECL_H(H)                                                            \
+  void plain_table_h##H(PlainLauncher (*row)[3], UnitLauncher* col, UnitLauncher* rowu); \
+  int merged_strip_cols_h##H();                                                      \
+  int merged_block_rows_w##H();
+BRIDCT_DECL_H(8)
+BRIDCT_DECL_H(16)
+BRIDCT_DECL_H(32)
+BRIDCT_DECL_H(64)
+BRIDCT_DECL_H(128)
+BRIDCT_DECL_H(256)
+BRIDCT_DECL_H(512)
+BRIDCT_DECL_H(1024)
+#undef BRIDCT_DECL_H
+
+int merged_strip_cols(int h) {
+  switch (h) {
+    case 32: return merged_strip_cols_h32();
+    case 64: return merged_strip_cols_h64();
+    case 128: return merged_strip_cols_h128();
+    case 256: return merged_strip_cols_h256();
+    case 512: return merged_strip_cols_h512();
+    case 1024: return merged_strip_cols_h1024();
+    default: return 0;
+  }
+}
+
+int merged_block_rows(int w) {
+  switch (w) {
+    case 32: return merged_block_rows_w32();
+    case 64: return merged_block_rows_w64();
+    case 128: return merged_block_rows_w128();
+    case 256: return merged_block_rows_w256();
+    case 512: return merged_block_rows_w512();
+    case 1024: return merged_block_rows_w1024();
+    default: return 0;
+  }
+}
 
 static std::mutex g_dev_mutex;
 static std::map<int, std::unique_ptr<DeviceCtx>> g_devices;
@@ -125,14 +154,14 @@ DeviceCtx* device_ctx(int device) {
   d->launch.sm_count = prop.multiProcessorCount;
   // Two-pass chunk: a quarter of L2 keeps the column pass's output resident for the row pass.
   PlainLauncher (*tab)[8][3] = d->plain;
-  plain_table_h8(tab[0]);
-  plain_table_h16(tab[1]);
-  plain_table_h32(tab[2]);
-  plain_table_h64(tab[3]);
-  plain_table_h128(tab[4]);
-  plain_table_h256(tab[5]);
-  plain_table_h512(tab[6]);
-  plain_table_h1024(tab[7]);
+  plain_table_h8(tab[0], d->col_units[0], d->row_units[0]);
+  plain_table_h16(tab[1], d->col_units[1], d->row_units[1]);
+  plain_table_h32(tab[2], d->col_units[2], d->row_units[2]);
+  plain_table_h64(tab[3], d->col_units[3], d->row_units[3]);
+  plain_table_h128(tab[4], d->col_units[4], d->row_units[4]);
+  plain_table_h256(tab[5], d->col_units[5], d->row_units[5]);
+  plain_table_h512(tab[6], d->col_units[6], d->row_units[6]);
+  plain_table_h1024(tab[7], d->col_units[7], d->row_units[7]);
   for (int i = 0; i < 4; ++i) {
     const int N = 128 << i;
     std::vector<float2> tw;

@@ -18,6 +18,8 @@ struct DeviceCtx {
   long long l2_bytes = 0;
   LaunchCtx launch{};
   PlainLauncher plain[8][8][3] = {};
+  UnitLauncher col_units[8][3] = {};    // merged column passes, by lg(column length) and mode
+  UnitLauncher row_units[8][3] = {};    // merged row passes, by lg(row length) and mode
   FourStepTables fourstep[4] = {};      // N = 128, 256, 512, 1024
   std::vector<void*> table_mem;
   FourStepTables tables(int n) const;

@@ -60,6 +60,15 @@ static cudaError_t launch_tiles(Kernel k, int smem, int bps, TileArgs a, const L
   return launch_pdl(k, (unsigned)grid, (unsigned)threads, smem, st, pdl, a);
 }
 
+// Route of an (H, W, MODE) batch: whole 32768-float arrays as single tiles in the modes where that
+// measured faster than two passes; other shapes above 16384 floats take the two passes.
+__host__ __device__ constexpr bool whole_array_route(int H, int W, int MODE) {
+  return H * W == 32768 && (MODE == LM_INV || H == 1024 || H == 64 || (H == 32 && MODE == LM_FWD));
+}
+__host__ __device__ constexpr bool two_pass_route(int H, int W, int MODE) {
+  return H * W > 16384 && !whole_array_route(H, W, MODE);
+}
+
 // GEN: the batch has general layouts (strided arrays or an offset table, BatchLayout); the same
 // geometry choices run the GEN instantiations of the kernels, except that 8x8 arrays take the
 // generic tile kernel instead of the dedicated one-thread-per-array kernels.
@@ -112,7 +121,7 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     const int bps = kernel_blocks_per_sm(k, smem, T);
     TileArgs a{x, y, (batch * H + TR - 1) / TR, batch * H, tab, lx, ly};
     return launch_tiles(k, smem, bps, a, ctx, st, T);
-  } else if constexpr (H * W == 32768 && (MODE == LM_INV || H == 1024 || H == 64 || (H == 32 && MODE == LM_FWD))) {
+  } else if constexpr (whole_array_route(H, W, MODE)) {
     // Whole 32768-float arrays as tiles (one CTA per SM, both passes in shared memory) instead of
     // the two passes, where that measured faster: every inverse (+5..21%), forward of 1024 x 32,
     // 32 x 1024 and 64 x 512 (+2..14%), round trips of 1024 x 32 and 64 x 512 (+2..6%); round
@@ -170,6 +179,38 @@ cudaError_t launch_plain(const float* x, float* y, long long batch, cudaStream_t
   if (lx && ly) return launch_plain_impl<H, W, MODE, true>(x, y, batch, st, tab, ctx, *lx, *ly);
   return launch_plain_impl<H, W, MODE, false>(x, y, batch, st, tab, ctx, BatchLayout{}, BatchLayout{});
 }
+
+// Merged passes of a ragged batch (UNITS kernels): one launch over the column strips of arrays of
+// column length H and any width (launch_col_units), or over the row blocks of arrays of row length
+// W and any height (launch_row_units), with the geometry the two-pass route uses for them (the
+// strip width depends only on H and the row-block height only on W for two-pass shapes; the
+// templates take 1024 for the other axis).  `units` lists the strips (or blocks), n of them.
+using UnitLauncher = cudaError_t (*)(const float*, float*, const PassUnit*, long long, cudaStream_t,
+                                     LineTables, const LaunchCtx&);
+
+template <int H, int MODE>
+cudaError_t launch_col_units(const float* x, float* y, const PassUnit* units, long long n, cudaStream_t st,
+                             LineTables tab, const LaunchCtx& ctx) {
+  using Gm = Geometry<H, 1024>;
+  constexpr int TC_T = H == 128 && MODE == LM_RT ? 128 : kThreads;
+  auto k = k_colstrip<H, 1024, Gm::kTC, MODE, TC_T, false, true>;
+  TileArgs a{x, y, n, n * H, tab, BatchLayout{}, BatchLayout{}, units};
+  return launch_tiles(k, Gm::kSmemStrip, kernel_blocks_per_sm(k, Gm::kSmemStrip, TC_T), a, ctx, st, TC_T, false);
+}
+
+template <int W, int MODE>
+cudaError_t launch_row_units(const float* x, float* y, const PassUnit* units, long long n, cudaStream_t st,
+                             LineTables tab, const LaunchCtx& ctx) {
+  using Gm = Geometry<1024, W>;
+  constexpr int TR_T = W == 128 && MODE == LM_RT ? 128 : kThreads;
+  auto k = k_full<1024, W, Gm::kRB, false, true, MODE, TR_T, false, true>;
+  TileArgs a{x, y, n, n * Gm::kRB, tab, BatchLayout{}, BatchLayout{}, units};
+  return launch_tiles(k, Gm::kSmemRows, kernel_blocks_per_sm(k, Gm::kSmemRows, TR_T), a, ctx, st, TR_T, false);
+}
+
+// Strip width of two-pass arrays of column length h, and row-block height of row length w.
+int merged_strip_cols(int h);
+int merged_block_rows(int w);
 
 // Per-H instantiation units (plain_inst.cu compiled once per H) export this table row.
 void plain_table_row(int h, PlainLauncher (*row)[3]);

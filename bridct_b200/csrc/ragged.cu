@@ -26,6 +26,16 @@ struct RaggedClass {
 
 constexpr int kRaggedMaxStreams = 8;
 
+// A merged pass: every column strip (col) or row block of the MERGED classes that share one column
+// length (or row length) and mode, as one launch over a device table of units.
+struct MergedPass {
+  int len = 0, mode = 0;
+  bool col = true;
+  bridct::PassUnit* d_units = nullptr;
+  long long n = 0;
+  size_t floats = 0;
+};
+
 struct bridct_ragged {
   int device = 0;
   bridct::DeviceCtx* dev = nullptr;
@@ -44,9 +54,11 @@ struct bridct_ragged {
   // shape classes, in decreasing size; classes scheduled as their own launches run on `streams`
   // side streams forked from and joined back into the caller's stream
   std::vector<RaggedClass> classes;
+  std::vector<MergedPass> merged;       // column passes first, then row passes
   int streams = 4;
   cudaStream_t aux[kRaggedMaxStreams] = {};
   cudaEvent_t fork_ev = nullptr, join_ev[kRaggedMaxStreams] = {};
+  cudaEvent_t mid_ev[kRaggedMaxStreams] = {}, mid_fork = nullptr;   // between merged column and row passes
 };
 
 namespace bridct {
@@ -161,11 +173,75 @@ int build_classes(bridct_ragged* r) {
     if (e != cudaSuccess) return cuda_fail(e, "ragged class tables");
   }
   cudaError_t e = cudaEventCreateWithFlags(&r->fork_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->mid_fork, cudaEventDisableTiming);
   for (int i = 0; e == cudaSuccess && i < kRaggedMaxStreams; ++i) {
     e = cudaStreamCreateWithFlags(&r->aux[i], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->join_ev[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->mid_ev[i], cudaEventDisableTiming);
   }
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "ragged streams");
+}
+
+void free_merged(bridct_ragged* r) {
+  for (MergedPass& m : r->merged) cudaFree(m.d_units);
+  r->merged.clear();
+}
+
+// Unit tables of the merged passes: column strips of the MERGED classes grouped by (column length,
+// mode), row blocks grouped by (row length, mode), each group largest first.
+int build_merged(bridct_ragged* r) {
+  free_merged(r);
+  std::map<std::pair<int, int>, std::vector<PassUnit>> cols, rows;
+  std::map<std::pair<int, int>, size_t> cfl, rfl;
+  for (const RaggedClass& c : r->classes) {
+    if (c.schedule != BRIDCT_RAGGED_MERGED) continue;
+    const int tc = merged_strip_cols(c.h), rb = merged_block_rows(c.w);
+    for (int i : c.arrays) {
+      const long long off = (long long)r->items[i].offset;
+      for (int s0 = 0; s0 < c.w; s0 += tc) cols[{c.h, c.mode}].push_back(PassUnit{off + s0, c.w});
+      for (int r0 = 0; r0 < c.h; r0 += rb) rows[{c.w, c.mode}].push_back(PassUnit{off + (long long)r0 * c.w, c.w});
+      cfl[{c.h, c.mode}] += (size_t)c.h * c.w;
+      rfl[{c.w, c.mode}] += (size_t)c.h * c.w;
+    }
+  }
+  for (int pass = 0; pass < 2; ++pass) {
+    auto& groups = pass == 0 ? cols : rows;
+    auto& fl = pass == 0 ? cfl : rfl;
+    std::vector<MergedPass> list;
+    for (auto& kv : groups) {
+      MergedPass m;
+      m.len = kv.first.first;
+      m.mode = kv.first.second;
+      m.col = pass == 0;
+      m.n = (long long)kv.second.size();
+      m.floats = fl[kv.first];
+      cudaError_t e = cudaMalloc((void**)&m.d_units, kv.second.size() * sizeof(PassUnit));
+      if (e == cudaSuccess)
+        e = cudaMemcpy(m.d_units, kv.second.data(), kv.second.size() * sizeof(PassUnit), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        cudaFree(m.d_units);
+        free_merged(r);
+        return cuda_fail(e, "merged pass tables");
+      }
+      list.push_back(m);
+    }
+    std::stable_sort(list.begin(), list.end(), [](const MergedPass& a, const MergedPass& b) { return a.floats > b.floats; });
+    r->merged.insert(r->merged.end(), list.begin(), list.end());
+  }
+  return BRIDCT_OK;
+}
+
+int launch_merged(bridct_ragged* r, const MergedPass& m, const float* x, float* y, cudaStream_t st) {
+  const int li = lg(m.len);
+  UnitLauncher fn = m.col ? r->dev->col_units[li][m.mode] : r->dev->row_units[li][m.mode];
+  if (!fn) {
+    set_error("ragged: no merged pass for this length");
+    return BRIDCT_INVALID_ARGUMENT;
+  }
+  // the line tables of the pass's own axis (the other axis's are not read)
+  LineTables tab{r->dev->tables(m.len), r->dev->tables(m.len)};
+  cudaError_t e = fn(x, y, m.d_units, m.n, st, tab, r->dev->launch);
+  return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "merged pass launch");
 }
 
 // One class as its own plain-form launch over the class's offset table.
@@ -284,11 +360,14 @@ BRIDCT_API void bridct_ragged_destroy(bridct_ragged* r) {
   cudaFree(r->d_err);
   for (auto& kv : r->plans) bridct_plan_destroy(kv.second);
   for (RaggedClass& c : r->classes) cudaFree(c.d_offs);
+  free_merged(r);
   for (int i = 0; i < kRaggedMaxStreams; ++i) {
     if (r->aux[i]) cudaStreamDestroy(r->aux[i]);
     if (r->join_ev[i]) cudaEventDestroy(r->join_ev[i]);
+    if (r->mid_ev[i]) cudaEventDestroy(r->mid_ev[i]);
   }
   if (r->fork_ev) cudaEventDestroy(r->fork_ev);
+  if (r->mid_fork) cudaEventDestroy(r->mid_fork);
   delete r;
 }
 
@@ -306,19 +385,45 @@ BRIDCT_API int bridct_ragged_apply_device(bridct_ragged* r, const float* x, floa
   // Classes with their own launches run on side streams forked from the caller's stream (largest
   // class first, round robin) and joined back into it; the queue's persistent kernel runs on the
   // caller's stream meanwhile.  Capturable: the fork and join are events on captured streams.
+  // MERGED classes run as merged column passes, then (after every column pass has finished) merged
+  // row passes, spread over the side streams; classes with their own launches follow on the same
+  // streams.
   std::vector<const RaggedClass*> own;
   for (const RaggedClass& c : r->classes)
-    if (c.schedule != BRIDCT_RAGGED_QUEUE) own.push_back(&c);
+    if (c.schedule == BRIDCT_RAGGED_CLASS_LAUNCH || c.schedule == BRIDCT_RAGGED_CLASS_LAUNCH_SMALL) own.push_back(&c);
+  size_t ncol = 0;
+  for (const MergedPass& m : r->merged) ncol += m.col ? 1 : 0;
+  const size_t nrow = r->merged.size() - ncol;
+  const size_t widest = std::max(own.size(), std::max(ncol, nrow));
   cudaError_t e = cudaSuccess;
-  const int nst = std::max(1, std::min(r->streams, (int)own.size()));
-  if (!own.empty()) {
+  const int nst = std::max(1, std::min(r->streams, (int)widest));
+  const bool fork = !own.empty() || !r->merged.empty();
+  if (fork) {
     e = cudaEventRecord(r->fork_ev, st);
     for (int i = 0; e == cudaSuccess && i < nst; ++i) e = cudaStreamWaitEvent(r->aux[i], r->fork_ev, 0);
     if (e != cudaSuccess) return cuda_fail(e, "ragged fork");
-    for (size_t k = 0; k < own.size(); ++k) {
-      const int s = launch_class(r, *own[k], own[k]->schedule, x, y, r->aux[k % nst]);
+  }
+  if (!r->merged.empty()) {
+    for (size_t k = 0; k < ncol; ++k) {
+      const int s = launch_merged(r, r->merged[k], x, y, r->aux[k % nst]);
       if (s) return s;
     }
+    // every row block needs its array's column strips: all side streams meet here
+    for (int i = 1; e == cudaSuccess && i < nst; ++i) {
+      e = cudaEventRecord(r->mid_ev[i], r->aux[i]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(r->aux[0], r->mid_ev[i], 0);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(r->mid_fork, r->aux[0]);
+    for (int i = 1; e == cudaSuccess && i < nst; ++i) e = cudaStreamWaitEvent(r->aux[i], r->mid_fork, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "ragged merged barrier");
+    for (size_t k = 0; k < nrow; ++k) {
+      const int s = launch_merged(r, r->merged[ncol + k], x, y, r->aux[k % nst]);
+      if (s) return s;
+    }
+  }
+  for (size_t k = 0; k < own.size(); ++k) {
+    const int s = launch_class(r, *own[k], own[k]->schedule, x, y, r->aux[k % nst]);
+    if (s) return s;
   }
   if (!r->units.empty()) {
     e = cudaMemsetAsync(r->d_counters, 0, (r->items.size() + 1) * sizeof(unsigned int), st);
@@ -338,7 +443,7 @@ BRIDCT_API int bridct_ragged_apply_device(bridct_ragged* r, const float* x, floa
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "k_ragged launch");
   }
-  for (int i = 0; !own.empty() && i < nst; ++i) {
+  for (int i = 0; fork && i < nst; ++i) {
     e = cudaEventRecord(r->join_ev[i], r->aux[i]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(st, r->join_ev[i], 0);
     if (e != cudaSuccess) return cuda_fail(e, "ragged join");
@@ -363,11 +468,17 @@ BRIDCT_API int bridct_ragged_class_info(const bridct_ragged* r, size_t cls, int*
 BRIDCT_API int bridct_ragged_set_schedule(bridct_ragged* r, const int* schedules, size_t count, int streams) {
   if (!r || count != r->classes.size() || (count && !schedules) || streams < 1 || streams > kRaggedMaxStreams)
     return BRIDCT_INVALID_ARGUMENT;
-  for (size_t i = 0; i < count; ++i)
-    if (schedules[i] < BRIDCT_RAGGED_QUEUE || schedules[i] > BRIDCT_RAGGED_CLASS_LAUNCH_SMALL) {
+  for (size_t i = 0; i < count; ++i) {
+    if (schedules[i] < BRIDCT_RAGGED_QUEUE || schedules[i] > BRIDCT_RAGGED_MERGED) {
       set_error("bridct_ragged_set_schedule: unknown schedule " + std::to_string(schedules[i]));
       return BRIDCT_INVALID_ARGUMENT;
     }
+    const RaggedClass& c = r->classes[i];
+    if (schedules[i] == BRIDCT_RAGGED_MERGED && !two_pass_route(c.h, c.w, c.mode)) {
+      set_error("bridct_ragged_set_schedule: class " + std::to_string(i) + " is not a two-pass shape");
+      return BRIDCT_INVALID_ARGUMENT;
+    }
+  }
   DeviceGuard guard(r->device);
   if (guard.status != cudaSuccess) return cuda_fail(guard.status, "cudaSetDevice(batch device)");
   cudaError_t e = cudaDeviceSynchronize();   // the old queue may still be in use
@@ -375,7 +486,8 @@ BRIDCT_API int bridct_ragged_set_schedule(bridct_ragged* r, const int* schedules
   for (size_t i = 0; i < count; ++i) r->classes[i].schedule = schedules[i];
   r->streams = streams;
   build_units(r);
-  const int s = upload(r);
+  int s = upload(r);
+  if (!s) s = build_merged(r);
   if (s) return s;
   const int bps = kernel_setup(reinterpret_cast<const void*>(k_ragged), kRaggedSmem, kRaggedThreads);
   r->grid = (int)std::min<long long>((long long)r->dev->sm_count * std::max(1, bps),

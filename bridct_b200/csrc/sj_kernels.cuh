@@ -49,6 +49,15 @@ struct BatchLayout {
   int small_units = 0;   // two-pass shapes: force the few-array geometry (one line group per warp)
 };
 
+// One unit of a merged launch (UNITS kernels): a column strip or a row block of some array of a
+// ragged batch, starting `off` floats into both x and y, rows `ld` floats apart.  A merged column
+// launch covers strips of arrays that share the column length but not the width; a merged row
+// launch covers row blocks of arrays that share the row length but not the height.
+struct PassUnit {
+  long long off;
+  long long ld;
+};
+
 struct TileArgs {
   const float* x;
   float* y;
@@ -56,6 +65,7 @@ struct TileArgs {
   long long rows_total;   // rows of the (batch*h) x w matrix covered by this launch
   LineTables tab;
   BatchLayout lx, ly;     // layouts of x and y (GEN kernels only)
+  const PassUnit* units = nullptr;   // UNITS kernels: one unit per tile
 };
 
 // Offset (floats) of row g of the (batch*H) x W row matrix in a general layout.
@@ -310,8 +320,10 @@ __device__ __forceinline__ void run_lines(float* tile, int nlines, int es, const
 
 // Full-width tiles: TR consecutive rows (of width W) of the batch viewed as a (B*H) x W
 // matrix.  With DO_COL the tile holds TR/H whole arrays.
-template <int H, int W, int TR, bool DO_COL, bool DO_ROW, int MODE, int THREADS = kThreads, bool GEN = false>
+template <int H, int W, int TR, bool DO_COL, bool DO_ROW, int MODE, int THREADS = kThreads, bool GEN = false,
+          bool UNITS = false>
 __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
+  static_assert(!UNITS || !DO_COL, "merged units are row blocks");
   constexpr int P = DO_COL ? pitch_of(H, W, true) : rowblock_pitch(W);
   constexpr int XB = (THREADS / 32) * cmax(DO_COL ? ExchangeFloats<H>::value : 0, DO_ROW ? ExchangeFloats<W>::value : 0);
   extern __shared__ float smem[];
@@ -336,16 +348,22 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
   constexpr bool kPrefetch = THREADS == kThreads && TR * W <= 16384 &&
                              (DO_COL ? DO_ROW && (H >= 128 || W >= 128) && !(W >= 256 && TR * W >= 16384)
                                      : (DO_ROW && W == 128));
-  // General layouts (GEN): row r of tile t is row t * TR + r of the batch's row matrix.
+  // General layouts (GEN): row r of tile t is row t * TR + r of the batch's row matrix.  Merged
+  // row blocks (UNITS): row r of tile t is row r of unit t.
   auto xrow = [&](long long t) {
-    return [&a, t](int r) { return a.x + layout_row<H>(a.lx, t * TR + r); };
+    return [&a, t](int r) {
+      return UNITS ? a.x + a.units[t].off + r * a.units[t].ld : a.x + layout_row<H>(a.lx, t * TR + r);
+    };
   };
   auto yrow = [&](long long t) {
-    return [&a, t](int r) { return a.y + layout_row<H>(a.ly, t * TR + r); };
+    return [&a, t](int r) {
+      return UNITS ? a.y + a.units[t].off + r * a.units[t].ld : a.y + layout_row<H>(a.ly, t * TR + r);
+    };
   };
+  constexpr bool kRows = GEN || UNITS;   // per-row addressing
   TileRegs<P, kPrefetch ? TR : 4, kPrefetch ? W : 4, THREADS> next;
   if (kPrefetch && blockIdx.x < a.ntiles) {
-    if constexpr (GEN) next.load_rows(xrow(blockIdx.x), rows_of(blockIdx.x));
+    if constexpr (kRows) next.load_rows(xrow(blockIdx.x), rows_of(blockIdx.x));
     else next.load(a.x + blockIdx.x * (long long)TR * W, W, rows_of(blockIdx.x));
   }
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
@@ -355,11 +373,11 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
       next.put(tile);
       __syncthreads();
       if (t + gridDim.x < a.ntiles) {
-        if constexpr (GEN) next.load_rows(xrow(t + gridDim.x), rows_of(t + gridDim.x));
+        if constexpr (kRows) next.load_rows(xrow(t + gridDim.x), rows_of(t + gridDim.x));
         else next.load(a.x + (t + gridDim.x) * (long long)TR * W, W, rows_of(t + gridDim.x));
       }
     } else {
-      if constexpr (GEN) tile_load_rows<P>(xrow(t), TR, W, tile, rows);
+      if constexpr (kRows) tile_load_rows<P>(xrow(t), TR, W, tile, rows);
       else tile_load<P>(a.x + t * (long long)TR * W, W, TR, W, tile, rows);
       __syncthreads();
     }
@@ -377,7 +395,7 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
           tile, TR, 1, [](int l) { return l * P; }, xbuf, trow);
       __syncthreads();
     }
-    if constexpr (GEN) tile_store_rows<P>(yrow(t), rows, W, tile);
+    if constexpr (kRows) tile_store_rows<P>(yrow(t), rows, W, tile);
     else tile_store<P>(a.y + t * (long long)TR * W, W, rows, W, tile);
     __syncthreads();
   }
@@ -399,7 +417,7 @@ template <int H, int TC> __host__ __device__ constexpr bool transposed_strip() {
 }
 __host__ __device__ constexpr int transposed_pitch(int h, int tc) { return h == 1024 ? 1028 : tc == 32 ? h + 17 : h + 4; }
 
-template <int H, int W, int TC, int MODE, int THREADS = kThreads, bool GEN = false>
+template <int H, int W, int TC, int MODE, int THREADS = kThreads, bool GEN = false, bool UNITS = false>
 __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
   constexpr bool kT = transposed_strip<H, TC>();
   constexpr int P = kT ? transposed_pitch(H, TC) : strip_pitch(H, TC);
@@ -412,23 +430,30 @@ __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
   // Strips of 128- and 256-point columns prefetch the next strip into registers during the
   // transform; longer columns keep their occupancy.
   constexpr bool kPrefetch = THREADS == kThreads && (H == 128 || H == 256);
-  const long long xp = GEN ? a.lx.ld : W, yp = GEN ? a.ly.ld : W;
+  // Strip t: its first element in x and y and the row pitch of its array.  Contiguous batches:
+  // strip t % STRIPS of array t / STRIPS; GEN: the same through the layouts; UNITS: unit t.
   auto xarr = [&](long long arr) { return GEN ? a.x + layout_row<H>(a.lx, arr * H) : a.x + arr * (long long)H * W; };
   auto yarr = [&](long long arr) { return GEN ? a.y + layout_row<H>(a.ly, arr * H) : a.y + arr * (long long)H * W; };
-  auto src = [&](long long t) { return xarr(t / STRIPS) + (t % STRIPS) * TC; };
+  auto src = [&](long long t) -> const float* {
+    return UNITS ? a.x + a.units[t].off : xarr(t / STRIPS) + (t % STRIPS) * TC;
+  };
+  auto dst = [&](long long t) -> float* {
+    return UNITS ? a.y + a.units[t].off : yarr(t / STRIPS) + (t % STRIPS) * TC;
+  };
+  auto xpitch = [&](long long t) -> long long { return UNITS ? a.units[t].ld : GEN ? a.lx.ld : W; };
+  auto ypitch = [&](long long t) -> long long { return UNITS ? a.units[t].ld : GEN ? a.ly.ld : W; };
   TileRegs<P, kPrefetch ? H : 4, kPrefetch ? TC : 4, THREADS> next;
-  if (kPrefetch && blockIdx.x < a.ntiles) next.load(src(blockIdx.x), xp, H);
+  if (kPrefetch && blockIdx.x < a.ntiles) next.load(src(blockIdx.x), xpitch(blockIdx.x), H);
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     if (t + gridDim.x >= a.ntiles) griddep_trigger();   // this CTA's last strip
-    const long long arr = t / STRIPS;
-    const int s = (int)(t % STRIPS);
+    const long long xp = xpitch(t), yp = ypitch(t);
     if constexpr (kPrefetch) {
       next.put(tile);
       __syncthreads();
-      if (t + gridDim.x < a.ntiles) next.load(src(t + gridDim.x), xp, H);
+      if (t + gridDim.x < a.ntiles) next.load(src(t + gridDim.x), xpitch(t + gridDim.x), H);
     } else if constexpr (kT) {
       // eight float4 loads in flight per thread before their transposing stores
-      const float* g = xarr(arr) + s * TC;
+      const float* g = src(t);
       constexpr int Q = TC / 4, kPer = H * Q / THREADS, kBatch = kPer < 8 ? kPer : 8;
       static_assert(kPer % kBatch == 0, "strip staging batches");
 #pragma unroll 1
@@ -450,7 +475,7 @@ __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
       }
       __syncthreads();
     } else {
-      tile_load<P>(xarr(arr) + s * TC, xp, H, TC, tile, H);
+      tile_load<P>(src(t), xp, H, TC, tile, H);
       __syncthreads();
     }
     if constexpr (kT) {
@@ -461,7 +486,7 @@ __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
     }
     __syncthreads();
     if constexpr (kT) {
-      float* g = yarr(arr) + s * TC;
+      float* g = dst(t);
       constexpr int Q = TC / 4;
       for (int i = threadIdx.x; i < H * Q; i += THREADS) {
         const int r = i / Q, c = (i % Q) * 4;
@@ -469,7 +494,7 @@ __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
             make_float4(tile[c * P + r], tile[(c + 1) * P + r], tile[(c + 2) * P + r], tile[(c + 3) * P + r]);
       }
     } else {
-      tile_store<P>(yarr(arr) + s * TC, yp, H, TC, tile);
+      tile_store<P>(dst(t), yp, H, TC, tile);
     }
     __syncthreads();
   }

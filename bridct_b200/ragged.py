@@ -30,7 +30,15 @@ def pack_offsets(shapes: Sequence[Tuple[int, int]]) -> Tuple[np.ndarray, int]:
     return offs, pos
 
 
-SCHEDULES = {"queue": 0, "launch": 1, "launch_small": 2}
+SCHEDULES = {"queue": 0, "launch": 1, "launch_small": 2, "merged": 3}
+
+
+def two_pass(h: int, w: int, mode: int) -> bool:
+    """Whether the plain form runs (h, w, mode) as a column pass then a row pass (the classes that
+    may take the "merged" schedule): every shape above 16384 floats except whole 32768-float
+    arrays in the modes where one tile measured faster (plain_launch.cuh, whole_array_route)."""
+    whole = h * w == 32768 and (mode == 1 or h in (1024, 64) or (h == 32 and mode == 0))
+    return h * w > 16384 and not whole
 
 
 class RaggedBatch:

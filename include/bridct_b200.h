@@ -160,7 +160,10 @@ BRIDCT_API int bridct_ragged_apply_device(bridct_ragged *batch, const float *inp
 enum bridct_ragged_schedule {
     BRIDCT_RAGGED_QUEUE = 0,               /* units in the persistent kernel's queue           */
     BRIDCT_RAGGED_CLASS_LAUNCH = 1,        /* the class's own fixed-shape launch               */
-    BRIDCT_RAGGED_CLASS_LAUNCH_SMALL = 2   /* the same with the few-array geometry (two-pass)  */
+    BRIDCT_RAGGED_CLASS_LAUNCH_SMALL = 2,  /* the same with the few-array geometry (two-pass)  */
+    BRIDCT_RAGGED_MERGED = 3               /* two-pass classes only: one column-pass launch per
+                                              (column length, mode) and one row-pass launch per
+                                              (row length, mode) over all MERGED classes      */
 };
 BRIDCT_API size_t bridct_ragged_class_count(const bridct_ragged *batch);
 /* Shape, mode, array count and schedule of class `cls` (any output pointer may be NULL). */

@@ -232,3 +232,55 @@ def test_tune_classes_returns_a_checked_schedule():
     ref = RaggedBatch(items).apply(x)
     torch.cuda.synchronize()
     close(got, ref, x, items, b)
+
+
+@pytest.mark.parametrize("streams", [1, 3, 8])
+def test_merged_schedule_matches_queue_and_fp64(streams):
+    """Two-pass classes in merged column and row passes (one launch per column length and mode,
+    then one per row length and mode), the others in the queue or their own launch."""
+    from bridct_b200.ragged import two_pass
+
+    items = random_batch(240, 21)
+    items += [(1024, 1024, 0), (1024, 512, 1), (512, 1024, 2), (256, 128, 0), (32, 1024, 2), (1024, 32, 1)]
+    b = RaggedBatch(items)
+    rng = np.random.default_rng(22)
+    x = torch.from_numpy(rng.uniform(-1, 1, b.span).astype(np.float32)).cuda()
+    ref = b.apply(x)
+    sched = {}
+    for i, c in enumerate(b.classes()):
+        sched[c["key"]] = "merged" if two_pass(c["h"], c["w"], c["mode"]) else ("launch" if i % 2 else "queue")
+    assert "merged" in sched.values()
+    m = RaggedBatch(items, schedule={"classes": sched, "streams": streams})
+    y = m.apply(x)
+    torch.cuda.synchronize()
+    assert not m.timed_out()
+    close(y, ref, x, items, b)
+    for i in range(0, len(items), 11):
+        h, w, mo = items[i]
+        xi, yi = b.unpack(x)[i].cpu().numpy(), b.unpack(y)[i].cpu().numpy()
+        assert O.rel_max_error(yi, O.fp64_apply(xi, mo), xi, output_scaled=True) <= TOL, (h, w, mo)
+    # captured and replayed
+    s = torch.cuda.Stream()
+    y2 = torch.full_like(x, float("nan"))
+    with torch.cuda.stream(s):
+        m.apply(x, y2, stream=s.cuda_stream)
+    s.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        m.apply(x, y2, stream=s.cuda_stream)
+    y2.fill_(float("nan"))
+    with torch.cuda.stream(s):
+        g.replay()
+    s.synchronize()
+    assert torch.equal(y2, y)
+
+
+def test_merged_schedule_rejects_single_pass_classes():
+    from bridct_b200 import _lib
+    import ctypes as C
+
+    b = RaggedBatch([(64, 64, 0), (1024, 1024, 0)])
+    cls = b.classes()
+    arr = (C.c_int * len(cls))(*[3 if c["h"] * c["w"] <= 16384 else 0 for c in cls])
+    assert _lib.lib().bridct_ragged_set_schedule(b._h, arr, len(cls), 2) == _lib.INVALID_ARGUMENT
+    assert "two-pass" in _lib.last_error()
