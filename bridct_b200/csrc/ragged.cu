@@ -240,7 +240,8 @@ int launch_merged(bridct_ragged* r, const MergedPass& m, const float* x, float* 
   }
   // the line tables of the pass's own axis (the other axis's are not read)
   LineTables tab{r->dev->tables(m.len), r->dev->tables(m.len)};
-  cudaError_t e = fn(x, y, m.d_units, m.n, st, tab, r->dev->launch);
+  // column passes read x and write y; row passes transform y in place
+  cudaError_t e = fn(m.col ? x : y, y, m.d_units, m.n, st, tab, r->dev->launch);
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "merged pass launch");
 }
 
