@@ -700,7 +700,8 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
             cls = per_class.classes()
             sched = {"streams": class_schedule.get("streams"),
                      "classes_by_schedule": {k: sum(1 for c in cls if c["schedule"] == v)
-                                             for k, v in (("queue", 0), ("launch", 1), ("launch_small", 2))}}
+                                             for k, v in (("queue", 0), ("launch", 1), ("launch_small", 2),
+                                                          ("merged", 3))}}
         print(json.dumps({
             "metric": METRIC, "value": head["gbs"], "unit": "GB/s", "n_gpus": world,
             "steps": head["steps"], "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
