@@ -11,13 +11,16 @@
 //
 // One pass is a GEMM with M = rows (tiles of 128), N = L, K = L.  Each CTA owns one N-block of
 // 64 output columns: its slice of C_L (64 x L, split into bf16 or tf32 parts, in the K-major
-// 128-byte-swizzled image the UMMA B operand reads) is loaded into shared memory once, and the
-// CTA streams M-tiles through a TMA ring in K-chunks (64 FP32 per row for BF16x3, 32 for TF32x3).
+// 128-byte-swizzled image the UMMA B operand reads) is loaded into shared memory once (L <= 256)
+// or arrives chunk by chunk with the ring (L = 512, 1024), and the CTA streams M-tiles through a
+// TMA ring in K-chunks (64 FP32 per row for BF16x3, 32 for TF32x3).  Rows of 8, 16 or 32 points
+// run as 64-float super-rows against a block-diagonal B (SUB).
 // Split precision as in the 8x8 forms: BF16x3 = six products of 3-way splits, TF32x3 = three
 // products of 2-way splits, all accumulated in FP32 in TMEM.
 //
 // Warp roles (512 threads):
-//   warp 0 lane 0  TMA producer: ring stage s <- K-chunk of an M-tile (waits stage_free)
+//   warp 0 lane 0  TMA producer: ring stage s <- K-chunk of an M-tile (+ the B chunk when
+//                  streamed; waits stage_free)
 //   warp 1 lane 0  MMA issuer: TMEM acc set t += splits(stage s, A buffer a) . B slice; commits
 //                  stage_free/a_free per chunk and acc_full after an M-tile's last chunk
 //   warp 2         TMEM allocator
