@@ -81,6 +81,7 @@ struct bridct_plan {
   cudaEvent_t pipe_ev[3][kPipeSlots] = {};   // [copied in, transformed, copied out][slot]
   float* d_batch = nullptr;    // slots x (in, out) x chunk
   float* pin_batch = nullptr;  // slots x (in, out) x chunk, pageable callers only
+  void* copyout = nullptr;     // per slot, the state of a pageable output's copy out (host_pipeline.cu)
   size_t chunk = 0;            // arrays per pipeline chunk
   // precision-form scratch (allocated on first use of a tensor-core form that is not given a
   // caller workspace); tc_mu serializes its (re)allocation

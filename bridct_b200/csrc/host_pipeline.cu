@@ -34,6 +34,54 @@ class CopyPool {
     return *pool;
   }
 
+  // A copy that runs entirely on the pool threads, started later (submit, e.g. from a CUDA host
+  // callback once the source has arrived) and waited for with wait().
+  struct Deferred {
+    std::mutex mu;
+    std::condition_variable cv;
+    size_t left = 0;
+    char* d = nullptr;
+    const char* s = nullptr;
+    size_t n = 0, step = 0, parts = 0;
+  };
+
+  void prepare(Deferred& c, void* dst, const void* src, size_t n) {
+    c.d = static_cast<char*>(dst);
+    c.s = static_cast<const char*>(src);
+    c.n = n;
+    c.parts = std::min<size_t>(threads_.size(), std::max<size_t>(1, n / kPiece));
+    c.step = (n / c.parts + 63) & ~size_t(63);
+    std::lock_guard<std::mutex> lock(c.mu);
+    c.left = c.parts;
+  }
+
+  // Queues the pieces of a prepared copy (no CUDA calls: safe inside a CUDA host callback).
+  void submit(Deferred& c) {
+    size_t skipped = 0;
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      for (size_t i = 0; i < c.parts; ++i) {
+        const size_t off = i * c.step;
+        if (off >= c.n) {
+          ++skipped;
+          continue;
+        }
+        jobs_.push_back(Job{c.d + off, c.s + off, std::min(c.step, c.n - off), nullptr, &c});
+      }
+    }
+    cv_.notify_all();
+    if (skipped) {
+      std::lock_guard<std::mutex> lock(c.mu);
+      c.left -= skipped;
+      if (c.left == 0) c.cv.notify_all();
+    }
+  }
+
+  static void wait(Deferred& c) {
+    std::unique_lock<std::mutex> lock(c.mu);
+    c.cv.wait(lock, [&] { return c.left == 0; });
+  }
+
   void copy(void* dst, const void* src, size_t n) {
     const size_t parts = std::min<size_t>(threads_.size() + 1, std::max<size_t>(1, n / kPiece));
     if (parts <= 1) {
@@ -52,7 +100,7 @@ class CopyPool {
           continue;
         }
         jobs_.push_back(Job{static_cast<char*>(dst) + off, static_cast<const char*>(src) + off,
-                            std::min(step, n - off), &call});
+                            std::min(step, n - off), &call, nullptr});
       }
     }
     cv_.notify_all();
@@ -74,7 +122,8 @@ class CopyPool {
     char* d;
     const char* s;
     size_t n;
-    Call* call;
+    Call* call;          // a synchronous copy's state, or
+    Deferred* deferred;  // a deferred copy's
   };
 
   CopyPool() : pid_(getpid()) {
@@ -94,8 +143,13 @@ class CopyPool {
         jobs_.pop_front();
       }
       memcpy(j.d, j.s, j.n);
-      std::lock_guard<std::mutex> lock(j.call->mu);
-      if (--j.call->left == 0) j.call->cv.notify_all();
+      if (j.call) {
+        std::lock_guard<std::mutex> lock(j.call->mu);
+        if (--j.call->left == 0) j.call->cv.notify_all();
+      } else {
+        std::lock_guard<std::mutex> lock(j.deferred->mu);
+        if (--j.deferred->left == 0) j.deferred->cv.notify_all();
+      }
     }
   }
 
@@ -107,6 +161,9 @@ class CopyPool {
 };
 
 void host_copy(void* dst, const void* src, size_t n) { CopyPool::get().copy(dst, src, n); }
+
+// CUDA host callback: the copy-out's device-to-host copy has finished, start its pool copy.
+static void CUDART_CB start_copy_out(void* p) { CopyPool::get().submit(*static_cast<CopyPool::Deferred*>(p)); }
 
 static constexpr size_t kChunkBytes = 8u << 20;      // staging per slot and direction
 static constexpr size_t kMinChunkBytes = 4u << 20;   // smallest chunk a call cuts
@@ -133,6 +190,7 @@ static int ensure_batch_staging(bridct_plan* p, bool need_pinned) {
     cudaError_t e = cudaHostAlloc((void**)&p->pin_batch, 2 * kSlots * p->chunk * per, cudaHostAllocDefault);
     if (e != cudaSuccess) return cuda_fail(e, "pinned batch staging");
   }
+  if (need_pinned && !p->copyout) p->copyout = new CopyPool::Deferred[kSlots];
   return BRIDCT_OK;
 }
 
@@ -163,8 +221,25 @@ int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, s
   cudaEvent_t* ev_in = p->pipe_ev[0];
   cudaEvent_t* ev_k = p->pipe_ev[1];
   cudaEvent_t* ev_out = p->pipe_ev[2];
-  size_t pending_off[kSlots] = {}, pending_n[kSlots] = {};
+  // A pageable output's copy out of a slot's pinned staging starts on the pool threads as soon as
+  // the slot's device-to-host copy has finished (a host callback on the copy-out stream), so copies
+  // out overlap the host's copies in; a slot is reused only after its copy out has completed.  The
+  // copies' state belongs to the plan, so a callback never outlives it; every exit from this
+  // function waits for the copies it started.
+  CopyPool::Deferred* outcopy = static_cast<CopyPool::Deferred*>(p->copyout);
   bool used[kSlots] = {}, pending[kSlots] = {};
+  struct Drain {
+    cudaStream_t ds;
+    CopyPool::Deferred* outcopy;
+    bool* pending;
+    ~Drain() {
+      bool any = false;
+      for (int i = 0; i < kSlots; ++i) any = any || pending[i];
+      if (!any || cudaStreamSynchronize(ds) != cudaSuccess) return;
+      for (int i = 0; i < kSlots; ++i)
+        if (pending[i]) CopyPool::wait(outcopy[i]);
+    }
+  } drain{p->aux[2], outcopy, pending};
   cudaError_t e = cudaSuccess;
   size_t ci = 0;
   std::vector<size_t> sizes;
@@ -178,10 +253,8 @@ int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, s
     float* sz = sy + cf;
     float* px = p->pin_batch ? p->pin_batch + (size_t)slot * 2 * cf : nullptr;
     float* py = px ? px + cf : nullptr;
-    if (pending[slot]) {        // the host copies the slot's previous output out of pinned staging
-      e = cudaEventSynchronize(ev_out[slot]);
-      if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");
-      host_copy(out + pending_off[slot], py, pending_n[slot]);
+    if (pending[slot]) {        // the slot's previous output has left its pinned staging
+      CopyPool::wait(outcopy[slot]);
       pending[slot] = false;
     }
     const float* kx;
@@ -232,9 +305,11 @@ int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, s
           e = cudaMemcpyAsync(out + off, sy, nbytes, cudaMemcpyDeviceToHost, ds);
         } else {
           e = cudaMemcpyAsync(py, sy, nbytes, cudaMemcpyDeviceToHost, ds);
-          pending_off[slot] = off;
-          pending_n[slot] = nbytes;
-          pending[slot] = true;
+          if (e == cudaSuccess) {
+            CopyPool::get().prepare(outcopy[slot], out + off, py, nbytes);
+            e = cudaLaunchHostFunc(ds, start_copy_out, &outcopy[slot]);
+            pending[slot] = e == cudaSuccess;
+          }
         }
       }
       if (e == cudaSuccess) e = cudaEventRecord(ev_out[slot], ds);
@@ -248,8 +323,11 @@ int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, s
   // copy out, so the last copy out (or, for a device output, the last transform) ends the call.
   e = cudaStreamSynchronize(dy_ok ? ks : ds);
   if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");
-  for (int slot = 0; slot < kSlots; ++slot)
-    if (pending[slot]) host_copy(out + pending_off[slot], p->pin_batch + (size_t)slot * 2 * cf + cf, pending_n[slot]);
+  for (int slot = 0; slot < kSlots; ++slot)   // the callbacks have run: wait for their copies
+    if (pending[slot]) {
+      CopyPool::wait(outcopy[slot]);
+      pending[slot] = false;
+    }
   return BRIDCT_OK;
 }
 
@@ -269,6 +347,8 @@ bridct_plan* thread_square_plan(int n) {
 }
 
 void release_plan_extras(bridct_plan* p) {
+  delete[] static_cast<CopyPool::Deferred*>(p->copyout);
+  p->copyout = nullptr;
   if (p->tc_mem) cudaFree(p->tc_mem);
   p->tc_mem = nullptr;
   for (auto& row : p->pipe_ev)
