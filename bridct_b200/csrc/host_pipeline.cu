@@ -190,7 +190,7 @@ static int ensure_batch_staging(bridct_plan* p, bool need_pinned) {
     cudaError_t e = cudaHostAlloc((void**)&p->pin_batch, 2 * kSlots * p->chunk * per, cudaHostAllocDefault);
     if (e != cudaSuccess) return cuda_fail(e, "pinned batch staging");
   }
-  if (need_pinned && !p->copyout) p->copyout = new CopyPool::Deferred[kSlots];
+  if (need_pinned && !p->copyout) p->copyout = new CopyPool::Deferred[2 * kSlots];   // copies out, copies in
   return BRIDCT_OK;
 }
 
@@ -226,24 +226,51 @@ int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, s
   // out overlap the host's copies in; a slot is reused only after its copy out has completed.  The
   // copies' state belongs to the plan, so a callback never outlives it; every exit from this
   // function waits for the copies it started.
+  // A pageable input's copy into a slot's pinned staging runs on the pool threads one chunk ahead:
+  // chunk k+1's copy is queued before the host waits for chunk k's, so the pool never idles
+  // between chunks.
   CopyPool::Deferred* outcopy = static_cast<CopyPool::Deferred*>(p->copyout);
-  bool used[kSlots] = {}, pending[kSlots] = {};
+  CopyPool::Deferred* incopy = outcopy ? outcopy + kSlots : nullptr;
+  bool used[kSlots] = {}, pending[kSlots] = {}, loading[kSlots] = {};
   struct Drain {
     cudaStream_t ds;
     CopyPool::Deferred* outcopy;
+    CopyPool::Deferred* incopy;
     bool* pending;
+    bool* loading;
     ~Drain() {
+      for (int i = 0; i < kSlots; ++i)
+        if (loading[i]) CopyPool::wait(incopy[i]);
       bool any = false;
       for (int i = 0; i < kSlots; ++i) any = any || pending[i];
       if (!any || cudaStreamSynchronize(ds) != cudaSuccess) return;
       for (int i = 0; i < kSlots; ++i)
         if (pending[i]) CopyPool::wait(outcopy[i]);
     }
-  } drain{p->aux[2], outcopy, pending};
+  } drain{p->aux[2], outcopy, incopy, pending, loading};
   cudaError_t e = cudaSuccess;
   size_t ci = 0;
   std::vector<size_t> sizes;
   for (size_t a = 0; a < batch; a += chunk) sizes.push_back(batch - a < chunk ? batch - a : chunk);
+  // queues chunk k's copy into its slot's pinned staging (after the slot's previous copy in has
+  // read it out)
+  auto queue_copy_in = [&](size_t k) -> cudaError_t {
+    const int sl = (int)(k % kSlots);
+    if (k >= (size_t)kSlots) {
+      const cudaError_t ee = cudaEventSynchronize(ev_in[sl]);
+      if (ee != cudaSuccess) return ee;
+    }
+    const size_t first = k * chunk;
+    CopyPool::get().prepare(incopy[sl], p->pin_batch + (size_t)sl * 2 * cf, in + first * per,
+                            sizes[k] * per * sizeof(float));
+    CopyPool::get().submit(incopy[sl]);
+    loading[sl] = true;
+    return cudaSuccess;
+  };
+  if (stage_in && !sizes.empty()) {
+    e = queue_copy_in(0);
+    if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");
+  }
   size_t a0 = 0;
   for (size_t na : sizes) {
     const int slot = (int)(ci % kSlots);
@@ -270,11 +297,12 @@ int host_batch_pipeline(bridct_plan* p, int mode, const float* in, float* out, s
       } else if (pin_in) {
         e = cudaMemcpyAsync(sx, in + off, nbytes, cudaMemcpyHostToDevice, hs);
       } else {
-        if (used[slot]) {      // px is free once the slot's last copy in has read it
-          e = cudaEventSynchronize(ev_in[slot]);
+        if (ci + 1 < sizes.size()) {   // the next chunk's copy in goes to the pool now
+          e = queue_copy_in(ci + 1);
           if (e != cudaSuccess) return cuda_fail(e, "batch pipeline");
         }
-        host_copy(px, in + off, nbytes);
+        CopyPool::wait(incopy[slot]);
+        loading[slot] = false;
         e = cudaMemcpyAsync(sx, px, nbytes, cudaMemcpyHostToDevice, hs);
       }
       if (e == cudaSuccess) e = cudaEventRecord(ev_in[slot], hs);
