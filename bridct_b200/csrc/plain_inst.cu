@@ -38,7 +38,9 @@ void BRIDCT_CAT(plain_table_h, BRIDCT_H)(PlainLauncher (*row)[3], UnitLauncher* 
 
 #if BRIDCT_H >= 32
 int BRIDCT_CAT(merged_strip_cols_h, BRIDCT_H)() { return Geometry<BRIDCT_H, 1024>::kTC; }
-int BRIDCT_CAT(merged_block_rows_w, BRIDCT_H)() { return Geometry<1024, BRIDCT_H>::kRB; }
+int BRIDCT_CAT(merged_block_rows_w, BRIDCT_H)() {
+  return Geometry<1024, BRIDCT_H>::kNarrowRows ? Geometry<1024, BRIDCT_H>::kRBn : Geometry<1024, BRIDCT_H>::kRB;
+}
 #else
 int BRIDCT_CAT(merged_strip_cols_h, BRIDCT_H)() { return 0; }
 int BRIDCT_CAT(merged_block_rows_w, BRIDCT_H)() { return 0; }

@@ -159,7 +159,11 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
       e = launch_tiles(kc, Gm::kSmemStrip, bpc, ac, ctx, st, TC_T, false);
     }
     if (e != cudaSuccess) return e;
-    if (nb * H / Gm::kRB < 2LL * ctx.sm_count || (GEN && lx.small_units)) {
+    if constexpr (Gm::kNarrowRows) {
+      auto krn = k_full<H, W, Gm::kRBn, false, true, MODE, 128, GEN>;
+      TileArgs ar{y, y, nb * H / Gm::kRBn, nb * H, tab, ly, ly};
+      e = launch_tiles(krn, Gm::kSmemRowsN, kernel_blocks_per_sm(krn, Gm::kSmemRowsN, 128), ar, ctx, st, 128, few);
+    } else if (nb * H / Gm::kRB < 2LL * ctx.sm_count || (GEN && lx.small_units)) {
       auto krs = k_full<H, W, Gm::kRBs, false, true, MODE, TR_T, GEN>;
       TileArgs ar{y, y, nb * H / Gm::kRBs, nb * H, tab, ly, ly};
       e = launch_tiles(krs, Gm::kSmemRowsS, kernel_blocks_per_sm(krs, Gm::kSmemRowsS, TR_T), ar, ctx, st, TR_T,
@@ -202,10 +206,16 @@ template <int W, int MODE>
 cudaError_t launch_row_units(const float* x, float* y, const PassUnit* units, long long n, cudaStream_t st,
                              LineTables tab, const LaunchCtx& ctx) {
   using Gm = Geometry<1024, W>;
-  constexpr int TR_T = W == 128 && MODE == LM_RT ? 128 : kThreads;
-  auto k = k_full<1024, W, Gm::kRB, false, true, MODE, TR_T, false, true>;
-  TileArgs a{x, y, n, n * Gm::kRB, tab, BatchLayout{}, BatchLayout{}, units};
-  return launch_tiles(k, Gm::kSmemRows, kernel_blocks_per_sm(k, Gm::kSmemRows, TR_T), a, ctx, st, TR_T, false);
+  if constexpr (Gm::kNarrowRows) {
+    auto k = k_full<1024, W, Gm::kRBn, false, true, MODE, 128, false, true>;
+    TileArgs a{x, y, n, n * Gm::kRBn, tab, BatchLayout{}, BatchLayout{}, units};
+    return launch_tiles(k, Gm::kSmemRowsN, kernel_blocks_per_sm(k, Gm::kSmemRowsN, 128), a, ctx, st, 128, false);
+  } else {
+    constexpr int TR_T = W == 128 && MODE == LM_RT ? 128 : kThreads;
+    auto k = k_full<1024, W, Gm::kRB, false, true, MODE, TR_T, false, true>;
+    TileArgs a{x, y, n, n * Gm::kRB, tab, BatchLayout{}, BatchLayout{}, units};
+    return launch_tiles(k, Gm::kSmemRows, kernel_blocks_per_sm(k, Gm::kSmemRows, TR_T), a, ctx, st, TR_T, false);
+  }
 }
 
 // Strip width of two-pass arrays of column length h, and row-block height of row length w.

@@ -566,6 +566,13 @@ struct Geometry {
   static constexpr int kSmemStripS = strip_smem(kTCs);
   static constexpr int kRBs = W >= 128 ? cmin(kRB, kWarps * lines_per_warp<W>()) : kRB;
   static constexpr int kSmemRowsS = rows_smem(kRBs);
+  // Row passes of 256- and 512-point lines in 128-thread CTAs: one line group per warp (16 or 8
+  // rows) and four warps' exchange buffers, 42-43 KB, so five CTAs (20 warps) share an SM where
+  // 256-thread CTAs of 64 or 32 rows fit two (16 warps).
+  static constexpr bool kNarrowRows = W == 256 || W == 512;
+  static constexpr int kRBn = lines_per_warp<W>() * 4;
+  static constexpr int kSmemRowsN =
+      (round4(kRBn * rowblock_pitch(W)) + round4(4 * ExchangeFloats<W>::value) + TableFloats<W>::value) * 4;
 };
 
 }  // namespace bridct
