@@ -403,19 +403,27 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
 
 // Column strips: H rows x TC columns of one array (row pitch W in global memory; ld of the
 // layouts with GEN).
-// Strips of 1024-point columns (8 wide) and 512-point columns (32 wide) are staged transposed:
-// column c of the strip is row c of the tile (pitch transposed_pitch), so the column lines run the
-// row-line code instead of a stride-pitch walk down the tile, whose stride-2 Makhoul gather is
-// 2-way bank-conflicted at any pitch.  1024: pitch 1028, the row blocks' pitch, with 64-bit paired
-// gathers.  512: pitch 529 (= 17 mod 32); the bank model (tests/test_bank_model.py) counts 158
-// wavefronts per warp for 512-point rows at that pitch against 190 for the 34-pitch column walk,
-// and the scalar gathers of a warp's two lines fall into even and odd banks.  The transposing
-// scalar stores of the staging are conflict-free at both pitches: a warp covers 32 / (TC / 4) rows
-// of TC / 4 float4 groups, and group q's stores land 4 q * pitch = q * 128 / TC (mod 32) banks apart.
-template <int H, int TC> __host__ __device__ constexpr bool transposed_strip() {
-  return (H == 1024 && TC == 8) || (H == 512 && TC == 32);
+// Strips of 1024-point columns (16 wide; 8 wide for calls on a few arrays) and 512-point columns
+// (32 wide) are staged transposed: column c of the strip is row c of the tile (pitch
+// transposed_pitch), so the column lines run the row-line code instead of a stride-pitch walk down
+// the tile, whose stride-2 Makhoul gather is 2-way bank-conflicted at any pitch.  1024: pitch 1026
+// (16 wide) or 1028 (8 wide) with 64-bit paired gathers; a warp holds one 1024-point line, so the
+// pitch only matters to the staging.  Sizing the 16-wide strip as transposed (114.6 KB, two CTAs
+// per SM) rather than at the column walk's pitch measured +1.4..4.6% on every 1024-high two-pass
+// shape over 8 wide strips (64-byte row segments instead of 32).  512: pitch 529 (= 17 mod 32); the
+// bank model (tests/test_bank_model.py) counts 158 wavefronts per warp for 512-point rows at that
+// pitch against 190 for the 34-pitch column walk, and the scalar gathers of a warp's two lines fall
+// into even and odd banks.  Narrower 512-point strips (8 wide, 128-thread CTAs, five per SM)
+// measured 20-25% slower: 32-byte row segments.  The transposing scalar stores of the staging are
+// conflict-free at these pitches: a warp covers 32 / (TC / 4) rows of TC / 4 float4 groups, and
+// group q's stores land 4 q * pitch = q * 128 / TC (mod 32) banks apart.
+__host__ __device__ constexpr bool is_transposed_strip(int h, int tc) {
+  return (h == 1024 && (tc == 8 || tc == 16)) || (h == 512 && tc == 32);
 }
-__host__ __device__ constexpr int transposed_pitch(int h, int tc) { return h == 1024 ? 1028 : tc == 32 ? h + 17 : h + 4; }
+template <int H, int TC> __host__ __device__ constexpr bool transposed_strip() { return is_transposed_strip(H, TC); }
+__host__ __device__ constexpr int transposed_pitch(int h, int tc) {
+  return h == 1024 ? (tc == 16 ? 1026 : 1028) : tc == 32 ? h + 17 : h + 4;
+}
 
 template <int H, int W, int TC, int MODE, int THREADS = kThreads, bool GEN = false, bool UNITS = false>
 __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
@@ -533,7 +541,7 @@ struct Geometry {
   static constexpr int kSmemWhole = full_smem(1);
   // 2-pass class
   static constexpr int strip_tile(int tc) {
-    return (H == 1024 && tc == 8) || (H == 512 && tc == 32) ? tc * transposed_pitch(H, tc) : H * strip_pitch(H, tc);
+    return is_transposed_strip(H, tc) ? tc * transposed_pitch(H, tc) : H * strip_pitch(H, tc);
   }
   static constexpr int strip_smem(int tc) {
     return (round4(strip_tile(tc)) + round4(kWarps * ExchangeFloats<H>::value) + TableFloats<H>::value) * 4;
@@ -545,7 +553,9 @@ struct Geometry {
   }
   static constexpr int pick_tc() {
     int tc = (16384 / H) < W ? (16384 / H) : W;
-    while (tc > cmax(4, lines_per_warp<H>()) && sizing_smem(tc) > kSmemTwoPerSM) tc /= 2;
+    while (tc > cmax(4, lines_per_warp<H>()) &&
+           (is_transposed_strip(H, tc) ? strip_smem(tc) : sizing_smem(tc)) > kSmemTwoPerSM)
+      tc /= 2;
     return tc;
   }
   static constexpr int kTC = pick_tc();

@@ -170,9 +170,13 @@ def test_paired_row_gather_has_no_conflicts():
 def test_transposed_512_point_strips():
     """512-point column strips (32 wide) are staged transposed at pitch 529: the column lines then
     walk as rows, which the model counts cheaper than the 34-pitch column walk, and the transposing
-    scalar stores of the staging (a warp: 4 rows x 8 float4 groups) are conflict-free."""
+    scalar stores of the staging (a warp: 4 rows x 8 float4 groups) are conflict-free; so are those
+    of the 1024-point strips, 16 wide at pitch 1026 and 8 wide at 1028 (not at each other's)."""
     assert four_step_wavefronts(16, 529, rows=True) < 0.9 * four_step_wavefronts(16, 34, rows=False)
-    for pitch, tc in ((529, 32), (1028, 8)):
+    for pitch, tc in ((529, 32), (1028, 8), (1026, 16)):
         q = tc // 4
         for j in range(4):
             assert wavefronts([(4 * (l % q) + j) * pitch + l // q for l in range(32)]) == 1
+    for pitch, tc in ((1028, 16), (1026, 8)):
+        q = tc // 4
+        assert max(wavefronts([(4 * (l % q) + j) * pitch + l // q for l in range(32)]) for j in range(4)) == 2
