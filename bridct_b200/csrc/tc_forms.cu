@@ -128,8 +128,8 @@ std::vector<uint8_t> b_image(int form, bool inverse) {
 struct TcDevice {
   void* images[3][2] = {};   // [form][inverse]
   void* pass_images[3][8][2] = {};   // [form][log2(points per row) - 3][inverse], built on first use
-  void* fp8_images[2][2] = {};       // [L == 256][inverse]: E4M3 codes of C or C^T
-  float* fp8_scales[2][2] = {};      // their 32x32 tile scales
+  void* fp8_images[8][2] = {};       // [log2(L) - 3][inverse]: E4M3 codes of C or C^T (block-diagonal below 128)
+  float* fp8_scales[8][2] = {};      // their 32x32 tile scales
   int* err = nullptr;
 };
 
@@ -238,14 +238,22 @@ uint8_t e4m3_encode(double v) {
   return (uint8_t)(best | (v < 0 && best ? 0x80 : 0));
 }
 
-// E4M3 image of C_L (forward) or C_L^T for the FP8 pass: slice nb (64 rows) at nb * 64 * L bytes,
-// laid out [K atom of 128][64 rows x 128 bytes, SW128]; scales [L/32 row bands][L/32 K-tiles].
+// E4M3 image of the FP8 pass's B for rows of L points: C_L (forward) or C_L^T, block-diagonal
+// with LS / L copies for super-rows of LS = max(L, 128) codes.  Slice nb (64 rows) at nb * 64 * LS
+// bytes, laid out [K atom of 128][64 rows x 128 bytes, SW128]; scales [LS/32 row bands][LS/32
+// K-tiles] (1 for the all-zero tiles off the diagonal).
 void fp8_image(int L, bool inverse, std::vector<uint8_t>& img, std::vector<float>& sc) {
   const std::vector<double> c = dct_matrix(L);
-  auto at = [&](int n, int k) { return inverse ? c[(size_t)k * L + n] : c[(size_t)n * L + k]; };
-  const int nt = L / 32;
+  const int LS = L < 128 ? 128 : L;
+  auto at = [&](int n, int k) {
+    if (n / L != k / L) return 0.0;
+    n %= L;
+    k %= L;
+    return inverse ? c[(size_t)k * L + n] : c[(size_t)n * L + k];
+  };
+  const int nt = LS / 32;
   sc.assign((size_t)nt * nt, 1.0f);
-  img.assign((size_t)L * L, 0);
+  img.assign((size_t)LS * LS, 0);
   for (int bn = 0; bn < nt; ++bn)
     for (int bk = 0; bk < nt; ++bk) {
       double amax = 0.0;
@@ -256,7 +264,7 @@ void fp8_image(int L, bool inverse, std::vector<uint8_t>& img, std::vector<float
       for (int i = 0; i < 32; ++i)
         for (int j = 0; j < 32; ++j) {
           const int n = bn * 32 + i, k = bk * 32 + j;
-          const size_t slice = (size_t)(n / 64) * 64 * L;
+          const size_t slice = (size_t)(n / 64) * 64 * LS;
           const size_t off = slice + (size_t)(k / 128) * 8192 + tc::sw128(n % 64, (k % 128) / 16) + (k % 16);
           img[off] = e4m3_encode(at(n, k) / s);
         }
@@ -347,6 +355,7 @@ int launch_fused64(const bridct_plan* p, bool inverse, const float* x, float* y,
 
 int log2i(int v);
 
+// E4M3 super-rows (rows x LS codes) viewed by TMA in boxes of 128 rows x 128 bytes.
 bool make_fp8_map(CUtensorMap* m, const uint8_t* ptr, size_t rows, int L) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return false;
@@ -361,7 +370,7 @@ bool make_fp8_map(CUtensorMap* m, const uint8_t* ptr, size_t rows, int L) {
 
 bool fp8_tables(TcDevice* d, int L, bool inverse, const uint4** img, const float** sc) {
   std::lock_guard<std::mutex> lock(g_tc_mutex);
-  const int li = L == 256 ? 1 : 0, iv = inverse ? 1 : 0;
+  const int li = log2i(L) - 3, iv = inverse ? 1 : 0;
   if (!d->fp8_images[li][iv]) {
     std::vector<uint8_t> im;
     std::vector<float> scl;
@@ -380,23 +389,26 @@ bool fp8_tables(TcDevice* d, int L, bool inverse, const uint4** img, const float
   return true;
 }
 
-template <int L>
+// One FP8 row pass over `rows` rows of L = LS / SUB codes (super-rows of SUB rows).
+template <int LS, int SUB, int UKT>
 int launch_fp8pass(const bridct_plan* p, bool inverse, const uint8_t* q, const float* sx, float* out, size_t rows,
                    int rshift, cudaStream_t st, TcDevice* d) {
-  using F = tc::Fp8Layout<L>;
-  auto k = tc::k_fp8pass<L>;
+  using F = tc::Fp8Layout<LS, SUB, UKT>;
+  constexpr int L = LS / SUB;
+  auto k = tc::k_fp8pass<LS, SUB, UKT>;
   if (kernel_setup(reinterpret_cast<const void*>(k), F::kDynamic, F::kThreads) <= 0)
     return cuda_fail(cudaErrorInvalidConfiguration, "k_fp8pass shared memory");
   const uint4* img = nullptr;
   const float* sc = nullptr;
   if (!fp8_tables(d, L, inverse, &img, &sc)) return cuda_fail(cudaGetLastError(), "FP8 coefficient upload");
   CUtensorMap m;
-  if (!make_fp8_map(&m, q, rows, L)) {
+  const size_t srows = (rows + SUB - 1) / SUB;
+  if (!make_fp8_map(&m, q, srows, LS)) {
     set_error("cuTensorMapEncodeTiled failed");
     return BRIDCT_DEVICE_ERROR;
   }
-  constexpr int kBlocks = L / 64;
-  const long long mtiles = (long long)((rows + tc::kRows - 1) / tc::kRows);
+  constexpr int kBlocks = LS / 64;
+  const long long mtiles = (long long)((srows + tc::kRows - 1) / tc::kRows);
   long long slots = p->dev->sm_count / kBlocks;
   if (slots > mtiles) slots = mtiles;
   if (slots < 1) slots = 1;
@@ -406,10 +418,15 @@ int launch_fp8pass(const bridct_plan* p, bool inverse, const uint8_t* q, const f
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_fp8pass launch");
 }
 
-// Quantizes the rows (nrows x L, 32-row bands) into E4M3 codes q and tile scales sx.
-int launch_quant8(const float* rows, uint8_t* q, float* sx, size_t nrows, int L, cudaStream_t st) {
-  const long long ntiles = (long long)(nrows / 32) * (L / 32);
-  tc::k_quant8<<<(unsigned)((ntiles + 7) / 8), 256, 0, st>>>(rows, q, sx, ntiles, L);
+// Quantizes the rows (nrows x L, arrays of 1 << rshift rows) into E4M3 codes q and scales sx of
+// min(R, 32) x min(L, 32) tiles, and zeroes the codes after the rows up to the end of the last
+// 128-code super-row.
+int launch_quant8(const float* rows, uint8_t* q, float* sx, size_t nrows, int L, int rshift, cudaStream_t st) {
+  const int tr_shift = rshift < 5 ? rshift : 5, tl = L < 32 ? L : 32;
+  const long long ntiles = (long long)(nrows >> tr_shift) * (L / tl);
+  const int sub = L < 128 ? 128 / L : 1;
+  const int pad = (int)(((nrows + sub - 1) / sub * sub - nrows) * L);
+  tc::k_quant8<<<(unsigned)((ntiles + 7) / 8), 256, 0, st>>>(rows, q, sx, ntiles, L, tr_shift, pad);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_quant8 launch");
 }
@@ -424,12 +441,20 @@ int fp8_transform(const bridct_plan* p, bool inverse, const float* src, float* d
                   cudaStream_t st, TcDevice* d) {
   const int h = p->h, w = p->w;
   auto pass = [&](int L, const uint8_t* q, const float* sx, float* out, size_t rows, int rshift) {
-    return L == 128 ? launch_fp8pass<128>(p, inverse, q, sx, out, rows, rshift, st, d)
-                    : launch_fp8pass<256>(p, inverse, q, sx, out, rows, rshift, st, d);
+    switch (L) {
+      case 8: return launch_fp8pass<128, 16, 4>(p, inverse, q, sx, out, rows, rshift, st, d);
+      case 16: return launch_fp8pass<128, 8, 4>(p, inverse, q, sx, out, rows, rshift, st, d);
+      case 32: return launch_fp8pass<128, 4, 4>(p, inverse, q, sx, out, rows, rshift, st, d);
+      case 64: return launch_fp8pass<128, 2, 4>(p, inverse, q, sx, out, rows, rshift, st, d);
+      case 128: return launch_fp8pass<128, 1, 4>(p, inverse, q, sx, out, rows, rshift, st, d);
+      case 256: return launch_fp8pass<256, 1, 8>(p, inverse, q, sx, out, rows, rshift, st, d);
+      case 512: return launch_fp8pass<512, 1, 4>(p, inverse, q, sx, out, rows, rshift, st, d);
+      default: return launch_fp8pass<1024, 1, 4>(p, inverse, q, sx, out, rows, rshift, st, d);
+    }
   };
-  int e = launch_quant8(src, s.q, s.sx, nb * h, w, st);
+  int e = launch_quant8(src, s.q, s.sx, nb * h, w, log2i(h), st);
   if (!e) e = pass(w, s.q, s.sx, s.t, nb * h, log2i(h));
-  if (!e) e = launch_quant8(s.t, s.q, s.sx, nb * w, h, st);
+  if (!e) e = launch_quant8(s.t, s.q, s.sx, nb * w, h, log2i(w), st);
   if (!e) e = pass(h, s.q, s.sx, dst, nb * w, log2i(w));
   return e;
 }
@@ -454,13 +479,16 @@ int fp8_refined(const bridct_plan* p, bool inverse, const float* src, float* dst
 // Arrays per chunk of the FP8 form.  Chunks of 256 MB: the twelve launches of a refined
 // transform dominate smaller chunks (2048 arrays of 256x256, same outputs: 16 MB 304 GB/s,
 // 32 MB 344, 64 MB 352-366, 256 MB 382, 1 GB 389); the scratch needs about 17 bytes per element
-// of a chunk.
+// of a chunk: four FP32 buffers, the E4M3 codes (plus one super-row of padding) and the tile
+// scales (at most one per 64 elements).
+size_t fp8_scale_floats(size_t ce) { return (ce / 64 + 256 + 63) & ~size_t(63); }
+
 size_t fp8_chunk(size_t elems, size_t batch, size_t* bytes) {
   size_t chunk = (size_t(256) << 20) / (elems * sizeof(float));
   if (chunk < 1) chunk = 1;
   if (chunk > batch) chunk = batch;
   const size_t ce = chunk * elems;
-  *bytes = 16 * ce + ce + 4 * (ce / 1024) + 4096;
+  *bytes = 16 * ce + 4 * fp8_scale_floats(ce) + ce + 1024;
   return chunk;
 }
 
@@ -494,7 +522,7 @@ int apply_fp8(bridct_plan* p, int mode, const float* x, float* y, size_t batch, 
   float* base = static_cast<float*>(scratch_for(p, workspace, need, &status));
   if (!base) return status;
   Fp8Scratch s{base, base + ce, base + 2 * ce, base + 3 * ce, base + 4 * ce, nullptr};
-  s.q = reinterpret_cast<uint8_t*>(s.sx + ce / 1024 + 256);
+  s.q = reinterpret_cast<uint8_t*>(s.sx + fp8_scale_floats(ce));
   for (size_t b0 = 0; b0 < batch; b0 += chunk) {
     const size_t nb = batch - b0 < chunk ? batch - b0 : chunk;
     const float* xc = x + b0 * elems;
@@ -622,10 +650,6 @@ int apply_tc_form(bridct_plan* p, int mode, int form, const float* x, float* y, 
   if (!p || !x || !y || mode < 0 || mode > 2 || batch == 0) return BRIDCT_INVALID_ARGUMENT;
   if (form != BRIDCT_FORM_TC_BF16X3 && form != BRIDCT_FORM_TC_TF32X3 && form != BRIDCT_FORM_TC_FP8) {
     set_error("unsupported execution form");
-    return BRIDCT_INVALID_ARGUMENT;
-  }
-  if (form == BRIDCT_FORM_TC_FP8 && !((p->h == 128 || p->h == 256) && (p->w == 128 || p->w == 256))) {
-    set_error("the FP8 form covers arrays whose axes are 128 or 256");
     return BRIDCT_INVALID_ARGUMENT;
   }
   const bool kron = p->h == 8 && p->w == 8;   // every other supported shape runs two row passes

@@ -1,17 +1,25 @@
-// FP8 (E4M3) tensor-core form with per-32x32-tile scaling, for axes of 128 and 256.
+// FP8 (E4M3) tensor-core form with per-tile scaling, for every axis from 8 to 1024.
 //
 // A 2D transform is two row passes, as in the split-precision forms, but the operands are
-// quantized instead of split: every 32x32 tile of the data gets its own scale
-// s = max|tile| / 448 (the largest finite E4M3 value) and is stored as E4M3 codes, and C (or
-// C^T) is quantized the same way on the host.  A row of length L spans L/32 K-tiles with
-// different scales, so each K-tile's product (one kind::f8f6f4 MMA, K = 32) accumulates in its
-// own TMEM block and the epilogue forms sum_t sX(row band, t) * sC(column band, t) * acc_t in
-// FP32.  One refinement step on the host side of the form recovers accuracy:
+// quantized instead of split: every tile of min(R, 32) rows x min(L, 32) columns of an array
+// (32 x 32 where both axes allow) gets its own scale s = max|tile| / 448 (the largest finite E4M3
+// value) and is stored as E4M3 codes, and C (or C^T) is quantized the same way on the host.
+// A row of length L spans L/32 K-tiles with different scales, so each K-tile's product (one
+// kind::f8f6f4 MMA, K = 32) accumulates in its own TMEM block and the epilogue forms
+// sum_t sX(row band, t) * sC(column band, t) * acc_t in FP32.  One refinement step on the host
+// side of the form recovers accuracy:
 //     Y = Y8 + FP8(X - DCT-III_fp32(Y8)),  with the residual taken in FP32 by the plain form.
 //
-// k_quant8: one warp per 32x32 tile (lane = tile row): warp max of |x|, scale, E4M3 codes.
-// k_fp8pass<L> (256 threads): warp 0 TMA producer (E4M3 rows, 128-byte boxes), warp 1 MMA
-// issuer, warp 2 TMEM allocator, warps 4-7 epilogue (scales, sum, transposed stores).
+// Rows shorter than 128 codes run as super-rows of LS = 128 codes (SUB = 128 / L consecutive
+// rows) against a block-diagonal B of SUB copies of C_L; a K-tile of a super-row then holds
+// 32 / L whole rows (L < 32) or a 32-column band of one row, of one scale tile either way.
+//
+// k_quant8: one warp per scale tile: warp max of |x|, scale, E4M3 codes.
+// k_fp8pass<LS, SUB, UKT> (256 threads): warp 0 TMA producer (E4M3 super-rows, 128-byte boxes),
+// warp 1 MMA issuer, warp 2 TMEM allocator, warps 4-7 epilogue (scales, sum, transposed stores).
+// The pipeline unit is one M-tile's UKT K-tiles (UKT * 32 codes of 128 super-rows): 128- and
+// 256-code rows take a whole row per unit, 512- and 1024-code rows stream 4 K-tiles per unit
+// through two TMEM accumulator sets while the epilogue sums the units of a tile in registers.
 #pragma once
 #include <cuda_fp8.h>
 
@@ -22,42 +30,52 @@ namespace tc {
 
 constexpr float kE4M3Max = 448.0f;
 
-// rows: nrows x L FP32 (arrays of R rows); q: E4M3 codes, same layout; scales: per array
-// [R/32][L/32].  ntiles = nrows/32 * L/32.
+// rows: nrows x L FP32 (arrays of R rows); q: E4M3 codes, same layout; scales: one per tile of
+// TR = 1 << tr_shift rows (TR = min(R, 32)) and TL = min(L, 32) columns, tile index
+// (row / TR) * (L / TL) + column / TL.  ntiles = nrows / TR * L / TL.  Block 0 also zeroes the
+// `pad` bytes after the codes, the tail of the pass's last (partial) super-row.
 __global__ void __launch_bounds__(256) k_quant8(const float* __restrict__ rows, uint8_t* __restrict__ q,
-                                                float* __restrict__ scales, long long ntiles, int L) {
+                                                float* __restrict__ scales, long long ntiles, int L, int tr_shift,
+                                                int pad) {
   const int lane = threadIdx.x & 31;
+  const int TL = L < 32 ? L : 32;
+  const int ql = TL == 8 ? 1 : TL == 16 ? 2 : 3;   // log2 of the float4 groups of a tile row
+  const long long total = ntiles << (tr_shift + (TL == 8 ? 3 : TL == 16 ? 4 : 5));
+  if (blockIdx.x == 0)
+    for (int i = threadIdx.x; i < pad; i += blockDim.x) q[total + i] = 0;
   const long long t = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
   if (t >= ntiles) return;
-  const int tiles_per_band = L / 32;
-  const long long band = t / tiles_per_band;      // 32-row band of the row matrix
-  const int kt = (int)(t % tiles_per_band);
-  const long long row = band * 32 + lane;
-  const float4* src = reinterpret_cast<const float4*>(rows + row * L + kt * 32);
-  float v[32];
+  const int per_band = L / TL;
+  const long long row0 = (t / per_band) << tr_shift;
+  const int col0 = (int)(t % per_band) * TL;
+  const int n4 = (1 << tr_shift) << ql;             // float4 groups of the tile (16..256)
+  float4 v[8];
   float amax = 0.0f;
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const float4 a = __ldg(src + i);
-    v[4 * i] = a.x; v[4 * i + 1] = a.y; v[4 * i + 2] = a.z; v[4 * i + 3] = a.w;
-    amax = fmaxf(amax, fmaxf(fmaxf(fabsf(a.x), fabsf(a.y)), fmaxf(fabsf(a.z), fabsf(a.w))));
+  for (int k = 0; k < 8; ++k) {
+    const int i = lane + 32 * k;
+    v[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (i < n4) {
+      v[k] = __ldg(reinterpret_cast<const float4*>(rows + (row0 + (i >> ql)) * L + col0 + ((i & ((1 << ql) - 1)) << 2)));
+      amax = fmaxf(amax, fmaxf(fmaxf(fabsf(v[k].x), fabsf(v[k].y)), fmaxf(fabsf(v[k].z), fabsf(v[k].w))));
+    }
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xFFFFFFFFu, amax, o));
   const float s = amax > 0.0f ? amax / kE4M3Max : 1.0f;
   const float inv = 1.0f / s;
-  uint32_t w[8];
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const __nv_fp8x2_storage_t lo = __nv_cvt_float2_to_fp8x2(make_float2(v[4 * i] * inv, v[4 * i + 1] * inv),
-                                                             __NV_SATFINITE, __NV_E4M3);
-    const __nv_fp8x2_storage_t hi = __nv_cvt_float2_to_fp8x2(make_float2(v[4 * i + 2] * inv, v[4 * i + 3] * inv),
-                                                             __NV_SATFINITE, __NV_E4M3);
-    w[i] = (uint32_t)lo | ((uint32_t)hi << 16);
+  for (int k = 0; k < 8; ++k) {
+    const int i = lane + 32 * k;
+    if (i < n4) {
+      const __nv_fp8x2_storage_t lo =
+          __nv_cvt_float2_to_fp8x2(make_float2(v[k].x * inv, v[k].y * inv), __NV_SATFINITE, __NV_E4M3);
+      const __nv_fp8x2_storage_t hi =
+          __nv_cvt_float2_to_fp8x2(make_float2(v[k].z * inv, v[k].w * inv), __NV_SATFINITE, __NV_E4M3);
+      *reinterpret_cast<uint32_t*>(q + (row0 + (i >> ql)) * L + col0 + ((i & ((1 << ql) - 1)) << 2)) =
+          (uint32_t)lo | ((uint32_t)hi << 16);
+    }
   }
-  uint4* dst = reinterpret_cast<uint4*>(q + row * L + kt * 32);
-  dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
-  dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
   if (lane == 0) scales[t] = s;
 }
 
@@ -77,20 +95,22 @@ __global__ void k_accumulate(float4* __restrict__ y, const float4* __restrict__ 
   }
 }
 
-template <int L>
+template <int LS, int SUB, int UKT>
 struct Fp8Layout {
   static constexpr int kThreads = 256;
-  static constexpr int kKT = L / 32;                  // K-tiles (one MMA and one accumulator each)
-  static constexpr int kAtoms = L / 128;              // 128-byte K atoms per row
-  static constexpr int kStageBytes = kAtoms * 16384;  // 128 rows x L codes
-  static constexpr int kBBytes = kAtoms * 8192;       // 64 rows x L codes
-  static constexpr int kSets = 2 * kKT * 64 <= 512 ? 2 : 1;   // TMEM accumulator sets
-  static constexpr int kTmemAlloc = kSets * kKT * 64 <= 256 ? 256 : 512;
-  static constexpr int kStages = 4;
+  static constexpr int L = LS / SUB;                  // row length
+  static constexpr int kKT = LS / 32;                 // K-tiles of a super-row (one MMA and accumulator each)
+  static constexpr int kUnits = kKT / UKT;            // pipeline units per M-tile
+  static constexpr int kStageBytes = (UKT / 4) * 16384;   // 128 super-rows x UKT * 32 codes
+  static constexpr int kBBytes = (LS / 128) * 8192;   // 64 rows x LS codes
+  static constexpr int kSets = 2 * UKT * 64 <= 512 ? 2 : 1;   // TMEM accumulator sets
+  static constexpr int kTmemAlloc = kSets * UKT * 64 <= 256 ? 256 : 512;
+  static constexpr int kStages = (196608 - kBBytes) / kStageBytes < 8 ? (196608 - kBBytes) / kStageBytes : 8;
   static constexpr int kBOff = kStages * kStageBytes;
   static constexpr int kScOff = kBOff + kBBytes;       // sC of this CTA's two column bands
   static constexpr int kBarOff = kScOff + 2 * kKT * 4 + 64;
   static constexpr int kDynamic = ((kBarOff + 255) / 256) * 256 + 256 + 1024;
+  static_assert(LS % 128 == 0 && kKT % UKT == 0 && UKT % 4 == 0, "FP8 pass geometry");
   static_assert(kDynamic <= 232448, "shared memory budget");
 };
 
@@ -104,16 +124,20 @@ __device__ __forceinline__ void umma_fp8(uint32_t tmem_d, uint64_t adesc, uint64
 // Instruction descriptor for kind::f8f6f4: D FP32, A and B E4M3 (format 0), K-major, M=128, N=64.
 constexpr uint32_t kFp8Idesc = (1u << 4) | ((64u >> 3) << 17) | ((uint32_t)(kRows >> 4) << 24);
 
-// xmap: (nrows x L) E4M3 rows (box 128 x 128 bytes, SWIZZLE_128B); sx: their tile scales
-// ([array][R/32][L/32]); bimage: kBlocks slices of 64 rows x L codes; sc: C's tile scales
-// [L/32 column bands][L/32 K-tiles]; out: FP32 arrays written transposed (R = 1 << rshift).
-template <int L>
+// xmap: (ceil(nrows / SUB) x LS) E4M3 super-rows (box 128 x 128 bytes, SWIZZLE_128B); sx: their
+// scale tiles (k_quant8's layout, tr_shift = min(rshift, 5)); bimage: LS/64 slices of 64 rows x
+// LS codes; sc: C's tile scales [LS/32 column bands][LS/32 K-tiles]; out: FP32 arrays written
+// transposed (R = 1 << rshift rows of length L in, L rows of length R out).
+template <int LS, int SUB, int UKT>
 __global__ void __launch_bounds__(256, 1)
     k_fp8pass(const __grid_constant__ CUtensorMap xmap, const float* __restrict__ sx, float* __restrict__ out,
               const uint4* __restrict__ bimage, const float* __restrict__ sc, long long nrows, int rshift,
               int* __restrict__ err) {
-  using F = Fp8Layout<L>;
-  constexpr int kBlocks = L / 64;
+  using F = Fp8Layout<LS, SUB, UKT>;
+  constexpr int L = F::L;
+  constexpr int kBlocks = LS / 64;
+  constexpr int kSpan = L > 32 ? L : 32;             // codes whose K-tiles feed one output column
+  constexpr int kBandsPerRow = L > 32 ? L / 32 : 1;  // scale tiles across a row
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const uint32_t sbase = smem_u32(base);
@@ -127,8 +151,10 @@ __global__ void __launch_bounds__(256, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nblk = blockIdx.x % kBlocks;
   const long long slot = blockIdx.x / kBlocks, nslots = gridDim.x / kBlocks;
-  const long long mtiles = (nrows + kRows - 1) / kRows;
+  const long long srows = (nrows + SUB - 1) / SUB;
+  const long long mtiles = (srows + kRows - 1) / kRows;
   const long long nlocal = slot < mtiles ? (mtiles - 1 - slot) / nslots + 1 : 0;
+  const long long nunits = nlocal * F::kUnits;
 
   if (tid == 0) {
     s_abort = 0;
@@ -160,37 +186,41 @@ __global__ void __launch_bounds__(256, 1)
   const uint32_t tmem_base = *tmem_slot;
   bool ok = true;
 
+  // Unit j: M-tile j / kUnits of this CTA, K-tiles (j % kUnits) * UKT ...; stage j % kStages,
+  // accumulator set j % kSets.
   if (warp == 0 && lane == 0) {
-    for (long long j = 0; j < nlocal && ok && !s_abort; ++j) {
-      const int s = (int)(j % F::kStages);
+    for (long long j = 0; j < nunits && ok && !s_abort; ++j) {
+      const int s = (int)(j % F::kStages), u = (int)(j % F::kUnits);
       ok = mbar_wait(stage_free + 8 * s, ((uint32_t)(j / F::kStages) & 1u) ^ 1u);
       if (!ok) break;
-      const int row0 = (int)((slot + j * nslots) * kRows);
+      const int row0 = (int)((slot + (j / F::kUnits) * nslots) * kRows);
       const uint32_t dst = sbase + s * F::kStageBytes;
       mbar_expect_tx(stage_full + 8 * s, F::kStageBytes);
 #pragma unroll
-      for (int a = 0; a < F::kAtoms; ++a) tma_load_2d(dst + a * 16384u, &xmap, a * 128, row0, stage_full + 8 * s);
+      for (int a = 0; a < UKT / 4; ++a)
+        tma_load_2d(dst + a * 16384u, &xmap, (u * (UKT / 4) + a) * 128, row0, stage_full + 8 * s);
     }
   } else if (warp == 1 && lane == 0) {
-    for (long long j = 0; j < nlocal && ok && !s_abort; ++j) {
-      const int s = (int)(j % F::kStages), t = F::kSets == 2 ? (int)(j & 1) : 0;
+    for (long long j = 0; j < nunits && ok && !s_abort; ++j) {
+      const int s = (int)(j % F::kStages), t = F::kSets == 2 ? (int)(j & 1) : 0, u = (int)(j % F::kUnits);
       const uint32_t ph_set = F::kSets == 2 ? (uint32_t)(j >> 1) & 1u : (uint32_t)j & 1u;
       ok = mbar_wait(stage_full + 8 * s, (uint32_t)(j / F::kStages) & 1u);
       if (ok) ok = mbar_wait(acc_free + 8 * t, ph_set ^ 1u);
       if (!ok) break;
       tc_fence_after();
       const uint32_t st = sbase + s * F::kStageBytes, sb = sbase + F::kBOff;
-      const uint32_t acc = tmem_base + (uint32_t)(t * F::kKT * 64);
+      const uint32_t acc = tmem_base + (uint32_t)(t * UKT * 64);
 #pragma unroll
-      for (int kt = 0; kt < F::kKT; ++kt) {   // 32 E4M3 (32 bytes) per MMA, its own accumulator
-        const uint32_t ka = (kt >> 2) * 16384u + (kt & 3) * 32u, kb = (kt >> 2) * 8192u + (kt & 3) * 32u;
+      for (int kt = 0; kt < UKT; ++kt) {   // 32 E4M3 (32 bytes) per MMA, its own accumulator
+        const int kg = u * UKT + kt;
+        const uint32_t ka = (kt >> 2) * 16384u + (kt & 3) * 32u, kb = (kg >> 2) * 8192u + (kg & 3) * 32u;
         umma_fp8(acc + kt * 64, sw128_desc(st + ka), sw128_desc(sb + kb), kFp8Idesc);
       }
       umma_commit(stage_free + 8 * s);
       umma_commit(acc_full + 8 * t);
     }
-    if (ok && nlocal > 0) {
-      const long long j = nlocal - 1;
+    if (ok && nunits > 0) {
+      const long long j = nunits - 1;
       const int s = (int)(j % F::kStages);
       ok = mbar_wait(stage_free + 8 * s, (uint32_t)(j / F::kStages) & 1u);
     }
@@ -198,9 +228,10 @@ __global__ void __launch_bounds__(256, 1)
     const uint32_t r = tid - 128;
     const uint32_t quarter = (uint32_t)(warp & 3) * 32u;
     const long long rmask = (1ll << rshift) - 1;
-    const int bands = (int)((1ll << rshift) / 32);
-    for (long long j = 0; j < nlocal; ++j) {
-      const int t = F::kSets == 2 ? (int)(j & 1) : 0;
+    const int tr_shift = rshift < 5 ? rshift : 5;
+    float v[64];
+    for (long long j = 0; j < nunits; ++j) {
+      const int t = F::kSets == 2 ? (int)(j & 1) : 0, u = (int)(j % F::kUnits);
       const uint32_t ph_set = F::kSets == 2 ? (uint32_t)(j >> 1) & 1u : (uint32_t)j & 1u;
       if (r == 0) s_ok = (!s_abort && mbar_wait(acc_full + 8 * t, ph_set)) ? 1 : 0;
       named_sync(1, 128);
@@ -209,26 +240,32 @@ __global__ void __launch_bounds__(256, 1)
         break;
       }
       tc_fence_after();
-      const long long g = (slot + j * nslots) * kRows + r;
-      const bool live = g < nrows;
-      const long long b = g >> rshift, h = g & rmask;
-      float rs[F::kKT];
+      const long long gs = (slot + (j / F::kUnits) * nslots) * kRows + r;   // this thread's super-row
+      // data scale of each of the unit's K-tiles: its first row and column band
+      float rs[UKT];
 #pragma unroll
-      for (int kt = 0; kt < F::kKT; ++kt)
-        rs[kt] = live ? __ldg(sx + (b * bands + (h >> 5)) * F::kKT + kt) : 0.0f;
-      float v[64];
-      const uint32_t taddr = tmem_base + (uint32_t)(t * F::kKT * 64) + (quarter << 16);
+      for (int kt = 0; kt < UKT; ++kt) {
+        const int kg = u * UKT + kt;
+        const long long g = gs * SUB + (kg * 32) / L;
+        rs[kt] = g < nrows ? __ldg(sx + (g >> tr_shift) * kBandsPerRow + kg % kBandsPerRow) : 0.0f;
+      }
+      const uint32_t taddr = tmem_base + (uint32_t)(t * UKT * 64) + (quarter << 16);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
+        // K-tiles that feed output columns nblk * 64 + q * 16 ... + 15 (one row of the super-row,
+        // or one 32-code group of rows): the others meet zeros of the block-diagonal B
+        const int lo = ((nblk * 64 + q * 16) / kSpan) * (kSpan / 32), hi = lo + kSpan / 32;
         float acc[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) acc[i] = 0.0f;
+        for (int i = 0; i < 16; ++i) acc[i] = u == 0 ? 0.0f : v[q * 16 + i];
 #pragma unroll
-        for (int kt = 0; kt < F::kKT; ++kt) {
+        for (int kt = 0; kt < UKT; ++kt) {
+          const int kg = u * UKT + kt;
+          if (kg < lo || kg >= hi) continue;
           float w[16];
           tmem_ld16(taddr + kt * 64 + q * 16, w);
           tmem_wait_ld();
-          const float f = rs[kt] * s_sc[(q >> 1) * F::kKT + kt];
+          const float f = rs[kt] * s_sc[(q >> 1) * F::kKT + kg];
 #pragma unroll
           for (int i = 0; i < 16; ++i) acc[i] = fmaf(f, w[i], acc[i]);
         }
@@ -238,10 +275,25 @@ __global__ void __launch_bounds__(256, 1)
       tc_fence_before();
       named_sync(1, 128);
       if (r == 0) mbar_arrive(acc_free + 8 * t);
-      if (live) {
-        float* dst = out + ((b * L + (long long)nblk * 64) << rshift) + h;
+      if (u == F::kUnits - 1) {
+        if constexpr (SUB == 1) {
+          if (gs < nrows) {
+            const long long b = gs >> rshift, h = gs & rmask;
+            float* dst = out + ((b * L + (long long)nblk * 64) << rshift) + h;
 #pragma unroll
-        for (int c = 0; c < 64; ++c) dst[(long long)c << rshift] = v[c];
+            for (int c = 0; c < 64; ++c) dst[(long long)c << rshift] = v[c];
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < 64; ++c) {
+            const int n = nblk * 64 + c;
+            const long long g = gs * SUB + n / L;
+            if (g < nrows) {
+              const long long b = g >> rshift, h = g & rmask;
+              out[((b * L + n % L) << rshift) + h] = v[c];
+            }
+          }
+        }
       }
     }
   }

@@ -20,8 +20,8 @@ enum bridct_form {
     BRIDCT_FORM_TC_BF16X3 = 1, /* tensor cores: 3-term bf16 split of X, 6 products, FP32 accumulation;
                                   all shapes (8x8 as one Kronecker GEMM, the rest as two row passes) */
     BRIDCT_FORM_TC_TF32X3 = 2, /* tensor cores: 2-term tf32 split of X and C, 3 products; all shapes */
-    BRIDCT_FORM_TC_FP8 = 3     /* FP8 E4M3, per-32x32-tile scales, + one FP32 refinement step;
-                                  arrays whose axes are 128 or 256 */
+    BRIDCT_FORM_TC_FP8 = 3     /* FP8 E4M3, per-tile scales (32x32, or the array's axis where
+                                  shorter), + one FP32 refinement step; all shapes */
 };
 
 /* Thread-local description of the last failure in this thread ("" if none). */

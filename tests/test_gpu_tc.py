@@ -68,16 +68,6 @@ def test_tc8_no_write_past_batch(form):
     assert torch.isfinite(y[:300]).all()
 
 
-@pytest.mark.parametrize("shape", [(16, 16), (32, 64), (512, 512), (8, 64), (1024, 128)])
-def test_fp8_form_rejects_other_shapes(shape):
-    L = _lib.lib()
-    plan = torch_api._plan(torch.cuda.current_device(), *shape)
-    x = torch.randn(4, *shape, device="cuda")
-    y = torch.empty_like(x)
-    st = L.bridct_plan_apply_form_device(plan, 0, _lib.FORM_TC_FP8, x.data_ptr(), y.data_ptr(), 4, None)
-    assert st == _lib.INVALID_ARGUMENT
-
-
 SEP_SHAPES = [(64, 64), (128, 128), (256, 256), (64, 256), (256, 64), (128, 64), (64, 128), (256, 128)]
 
 # The TF32x3 round trip runs four tensor-core passes; the FP32 accumulation of the K = 8 tf32
@@ -192,18 +182,54 @@ def test_fp8_impulse_constant_and_batch_edges():
         assert O.rel_max_error(y[i:i + 1], ref[i:i + 1], x[i:i + 1], output_scaled=True) <= FP8_MAX, i
 
 
-def test_fp8_no_write_past_batch_and_rejects_other_shapes():
+@pytest.mark.parametrize("shape", [(128, 256), (8, 8), (8, 16), (16, 8), (8, 1024), (1024, 8)])
+def test_fp8_no_write_past_batch(shape):
+    # short rows run as 128-code super-rows of several rows (8-point rows: 16, two 8x8 arrays):
+    # an odd batch ends in a partial super-row whose missing rows must not be written
     L = _lib.lib()
-    plan = torch_api._plan(torch.cuda.current_device(), 128, 256)
-    x = torch.randn(4, 128, 256, device="cuda")
+    plan = torch_api._plan(torch.cuda.current_device(), *shape)
+    x = torch.randn(4, *shape, device="cuda")
     y = torch.full_like(x, 12345.0)
-    assert L.bridct_plan_apply_form_device(plan, 0, _lib.FORM_TC_FP8, x.data_ptr(), y.data_ptr(), 3, None) == 0
+    for mode in range(3):
+        assert L.bridct_plan_apply_form_device(plan, mode, _lib.FORM_TC_FP8, x.data_ptr(), y.data_ptr(), 3,
+                                               None) == 0
+        torch.cuda.synchronize()
+        assert (y[3] == 12345.0).all() and torch.isfinite(y[:3]).all(), (shape, mode)
+    assert L.bridct_plan_apply_form_device(plan, 0, _lib.FORM_TC_FP8, x.data_ptr(), x.data_ptr(), 1,
+                                           None) == _lib.OVERLAPPING_BUFFERS
+
+
+FP8_SHAPES = [(h, w) for h in (8, 16, 32, 64, 128, 256, 512, 1024) for w in (8, 16, 32, 64, 128, 256, 512, 1024)]
+
+
+@pytest.mark.parametrize("shape", FP8_SHAPES)
+def test_fp8_every_shape(shape):
+    """The FP8 form (min(R,32) x min(L,32) tile scales, one refinement step) on every shape, with
+    odd batches (partial 128-row tiles and partial super-rows), against float64."""
+    h, w = shape
+    batch = 2 if h * w >= 262144 else 3 if h * w >= 16384 else 37
+    x = np.random.default_rng(h * 5 + w).uniform(-1, 1, (batch, h, w)).astype(np.float32)
+    for mode in range(3):
+        y = run(x, mode, "tc_fp8")
+        ref = O.fp64_apply(x, mode)
+        k = 2.0 if mode == 2 else 1.0
+        assert O.rel_max_error(y, ref, x, output_scaled=True) <= k * FP8_MAX, (shape, mode)
+        assert O.rel_rms_error(y, ref, x) <= k * FP8_RMS, (shape, mode)
+
+
+@pytest.mark.parametrize("shape", [(8, 8), (8, 64), (32, 16)])
+def test_fp8_packed_rows_are_independent_of_the_batch_cut(shape):
+    """Arrays that share a super-row (several short rows in 128 codes, here across arrays) give
+    the same bits when transformed alone: the block-diagonal B keeps them apart, and the scales
+    are per array tile."""
+    x = torch.randn(101, *shape, device="cuda")
+    x[7] *= 1e5
+    y = torch_api.apply(x, 0, form="tc_fp8")
+    part = torch_api.apply(x[5:10].clone(), 0, form="tc_fp8")
+    one = torch_api.apply(x[8:9].clone(), 0, form="tc_fp8")
     torch.cuda.synchronize()
-    assert (y[3] == 12345.0).all() and torch.isfinite(y[:3]).all()
-    plan64 = torch_api._plan(torch.cuda.current_device(), 64, 64)
-    z = torch.randn(2, 64, 64, device="cuda")
-    assert L.bridct_plan_apply_form_device(plan64, 0, _lib.FORM_TC_FP8, z.data_ptr(), z.data_ptr() + 0, 1,
-                                           None) in (_lib.INVALID_ARGUMENT, _lib.OVERLAPPING_BUFFERS)
+    assert torch.equal(y[5:10], part)
+    assert torch.equal(y[8:9], one)
 
 
 def test_fp8_batch_across_chunks_matches_small_batches_bitwise():
