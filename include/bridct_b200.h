@@ -195,11 +195,10 @@ BRIDCT_API int bridct_ragged_set_wait_limit(bridct_ragged *batch, unsigned polls
  * static device array of about 0.9 MB that every GPU loading this library holds until exit.
  * Limits: at most 4096 arrays and 49152 work units per call (default unit geometry), else
  * BRIDCT_INVALID_ARGUMENT with a message.  A successful call allocates nothing.  The first call
- * on a device resolves that array's address and uploads the four-step tables into it, so make
- * it before any stream capture.  Every call shares the array and overwrites the previous call's
- * queue; calls are serialized and synchronous (they return after their kernel finished),
- * because two calls overlapping on the GPU would race on it.  Returns BRIDCT_TIMEOUT if a
- * bounded dependency wait expired. */
+ * on a device resolves that array's address and uploads the four-step tables into it.  Every
+ * call shares the array and overwrites the previous call's queue; calls are serialized and
+ * synchronous (they return after their kernel finished), because two calls overlapping on the
+ * GPU would race on it.  Returns BRIDCT_TIMEOUT if a bounded dependency wait expired. */
 BRIDCT_API int bridct_ragged_apply_noalloc(const bridct_ragged_item *items, size_t count,
                                            const float *input, float *output, void *stream);
 
