@@ -404,6 +404,11 @@ __global__ void __launch_bounds__(kTc8Threads, 1) k_tc8(const __grid_constant__ 
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
   bool ok = true;
+  // Launched with programmatic stream serialization: the prologue above (barriers, TMEM, the B
+  // image, which no kernel writes) overlaps the previous grid's tail; X and Y are touched only
+  // after the wait.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   if (warp == 0 && lane == 0) {
     for (int j = 0; j < ntile_local && ok && !s_abort; ++j) {

@@ -325,9 +325,8 @@ int launch_pass(const bridct_plan* p, bool inverse, const float* x, float* out, 
   long long slots = p->dev->sm_count / PL::kBlocks;
   if (slots > mtiles) slots = mtiles;
   if (slots < 1) slots = 1;
-  k<<<(unsigned)(slots * PL::kBlocks), tc::kPassThreads, PL::kDynamic, st>>>(xm, out, img, (long long)srows, rshift,
-                                                                         d->err);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_pdl(k, (unsigned)(slots * PL::kBlocks), tc::kPassThreads, PL::kDynamic, st, true, xm, out,
+                             img, (long long)srows, rshift, d->err);
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_tcpass launch");
 }
 
@@ -346,8 +345,8 @@ int launch_fused64(const bridct_plan* p, bool inverse, const float* x, float* y,
   }
   const long long tiles = (long long)((batch + 1) / 2);
   const long long grid = tiles < p->dev->sm_count ? tiles : p->dev->sm_count;
-  tc::k_tc64<<<(unsigned)grid, F::kThreads, F::kDynamic, st>>>(xm, y, img, (long long)batch, d->err);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_pdl(tc::k_tc64, (unsigned)grid, F::kThreads, F::kDynamic, st, true, xm, y, img,
+                             (long long)batch, d->err);
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_tc64 launch");
 }
 
@@ -412,9 +411,8 @@ int launch_fp8pass(const bridct_plan* p, bool inverse, const uint8_t* q, const f
   long long slots = p->dev->sm_count / kBlocks;
   if (slots > mtiles) slots = mtiles;
   if (slots < 1) slots = 1;
-  k<<<(unsigned)(slots * kBlocks), F::kThreads, F::kDynamic, st>>>(m, sx, out, img, sc, (long long)rows, rshift,
-                                                                    d->err);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_pdl(k, (unsigned)(slots * kBlocks), F::kThreads, F::kDynamic, st, true, m, sx, out, img, sc,
+                             (long long)rows, rshift, d->err);
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_fp8pass launch");
 }
 
@@ -623,9 +621,8 @@ int launch_tc8(const bridct_plan* p, int inverse, const float* x, float* y, size
   const int ntiles = (int)((batch + tc::kRows - 1) / tc::kRows);
   int grid = p->dev->sm_count * bps;
   if (grid > ntiles) grid = ntiles;
-  k<<<grid, tc::kTc8Threads, L::kDynamic, st>>>(xm, ym, reinterpret_cast<const uint4*>(d->images[FORM][inverse]),
-                                               ntiles, d->err);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_pdl(k, (unsigned)grid, tc::kTc8Threads, L::kDynamic, st, true, xm, ym,
+                             reinterpret_cast<const uint4*>(d->images[FORM][inverse]), ntiles, d->err);
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_tc8 launch");
 }
 

@@ -185,6 +185,11 @@ __global__ void __launch_bounds__(256, 1)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
   bool ok = true;
+  // Launched with programmatic stream serialization: the prologue above (barriers, TMEM, the
+  // coefficient image, which no kernel writes) overlaps the previous grid's tail; the data is
+  // touched only after the wait.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   // Unit j: M-tile j / kUnits of this CTA, K-tiles (j % kUnits) * UKT ...; stage j % kStages,
   // accumulator set j % kSets.

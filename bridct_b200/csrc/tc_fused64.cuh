@@ -113,6 +113,11 @@ __global__ void __launch_bounds__(Fused64::kThreads, 1)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
   bool ok = true;
+  // Launched with programmatic stream serialization: the prologue above (barriers, TMEM, the
+  // coefficient image, which no kernel writes) overlaps the previous grid's tail; the data is
+  // touched only after the wait.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   if (warp == 0 && lane == 0) {
     // The two-stage ring alone would expose a full DRAM latency per tile; tiles up to

@@ -248,6 +248,11 @@ __global__ void __launch_bounds__(kPassThreads, 1)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
   bool ok = true;
+  // Launched with programmatic stream serialization: the prologue above (barriers, TMEM, the
+  // coefficient image, which no kernel writes) overlaps the previous grid's tail; the data is
+  // touched only after the wait.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   if (warp == 0 && lane == 0) {
     for (long long j = 0; j < nchunk_local && ok && !s_abort; ++j) {
