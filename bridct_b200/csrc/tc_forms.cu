@@ -424,7 +424,9 @@ int launch_quant8(const float* rows, uint8_t* q, float* sx, size_t nrows, int L,
   const long long ntiles = (long long)(nrows >> tr_shift) * (L / tl);
   const int sub = L < 128 ? 128 / L : 1;
   const int pad = (int)(((nrows + sub - 1) / sub * sub - nrows) * L);
-  tc::k_quant8<<<(unsigned)((ntiles + 7) / 8), 256, 0, st>>>(rows, q, sx, ntiles, L, tr_shift, pad);
+  const long long per_block = 8LL * tc::quant8_tiles_per_warp(tr_shift, L);
+  tc::k_quant8<<<(unsigned)((ntiles + per_block - 1) / per_block), 256, 0, st>>>(rows, q, sx, ntiles, L, tr_shift,
+                                                                                  pad);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? BRIDCT_OK : cuda_fail(e, "k_quant8 launch");
 }

@@ -32,41 +32,48 @@ constexpr float kE4M3Max = 448.0f;
 
 // rows: nrows x L FP32 (arrays of R rows); q: E4M3 codes, same layout; scales: one per tile of
 // TR = 1 << tr_shift rows (TR = min(R, 32)) and TL = min(L, 32) columns, tile index
-// (row / TR) * (L / TL) + column / TL.  ntiles = nrows / TR * L / TL.  Block 0 also zeroes the
-// `pad` bytes after the codes, the tail of the pass's last (partial) super-row.
+// (row / TR) * (L / TL) + column / TL.  ntiles = nrows / TR * L / TL.  A tile's 16..256 float4
+// groups go to 32 lanes, or to 16 when it has only 16 (8 x 8 tiles: two tiles per warp).  Block 0
+// also zeroes the `pad` bytes after the codes, the tail of the pass's last (partial) super-row.
+__host__ __device__ constexpr int quant8_tiles_per_warp(int tr_shift, int L) {
+  return tr_shift + (L < 32 ? (L == 8 ? 1 : 2) : 3) < 5 ? 2 : 1;
+}
+
 __global__ void __launch_bounds__(256) k_quant8(const float* __restrict__ rows, uint8_t* __restrict__ q,
                                                 float* __restrict__ scales, long long ntiles, int L, int tr_shift,
                                                 int pad) {
   const int lane = threadIdx.x & 31;
-  const int TL = L < 32 ? L : 32;
-  const int ql = TL == 8 ? 1 : TL == 16 ? 2 : 3;   // log2 of the float4 groups of a tile row
-  const long long total = ntiles << (tr_shift + (TL == 8 ? 3 : TL == 16 ? 4 : 5));
+  const int tl_shift = L == 8 ? 3 : L == 16 ? 4 : 5;          // TL = min(L, 32)
+  const int ql = tl_shift - 2;                                  // float4 groups of a tile row
+  const int n4_shift = tr_shift + ql;                           // float4 groups of a tile (16..256)
+  const int lpt_shift = n4_shift < 5 ? n4_shift : 5;            // lanes per tile
+  const int bands_shift = (31 - __clz(L)) - tl_shift;           // tiles across a row
+  const long long total = ntiles << (tr_shift + tl_shift);
   if (blockIdx.x == 0)
     for (int i = threadIdx.x; i < pad; i += blockDim.x) q[total + i] = 0;
-  const long long t = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-  if (t >= ntiles) return;
-  const int per_band = L / TL;
-  const long long row0 = (t / per_band) << tr_shift;
-  const int col0 = (int)(t % per_band) * TL;
-  const int n4 = (1 << tr_shift) << ql;             // float4 groups of the tile (16..256)
+  const long long t = ((((long long)blockIdx.x << 3) + (threadIdx.x >> 5)) << (5 - lpt_shift)) + (lane >> lpt_shift);
+  const int sl = lane & ((1 << lpt_shift) - 1);
+  const bool live = t < ntiles;
+  const long long row0 = (t >> bands_shift) << tr_shift;
+  const int col0 = (int)(t & ((1 << bands_shift) - 1)) << tl_shift;
+  const int n4 = live ? 1 << n4_shift : 0;
   float4 v[8];
   float amax = 0.0f;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const int i = lane + 32 * k;
+    const int i = sl + (k << lpt_shift);
     v[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (i < n4) {
       v[k] = __ldg(reinterpret_cast<const float4*>(rows + (row0 + (i >> ql)) * L + col0 + ((i & ((1 << ql) - 1)) << 2)));
       amax = fmaxf(amax, fmaxf(fmaxf(fabsf(v[k].x), fabsf(v[k].y)), fmaxf(fabsf(v[k].z), fabsf(v[k].w))));
     }
   }
-#pragma unroll
-  for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xFFFFFFFFu, amax, o));
+  for (int o = (1 << lpt_shift) >> 1; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xFFFFFFFFu, amax, o));
   const float s = amax > 0.0f ? amax / kE4M3Max : 1.0f;
   const float inv = 1.0f / s;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const int i = lane + 32 * k;
+    const int i = sl + (k << lpt_shift);
     if (i < n4) {
       const __nv_fp8x2_storage_t lo =
           __nv_cvt_float2_to_fp8x2(make_float2(v[k].x * inv, v[k].y * inv), __NV_SATFINITE, __NV_E4M3);
@@ -76,7 +83,7 @@ __global__ void __launch_bounds__(256) k_quant8(const float* __restrict__ rows, 
           (uint32_t)lo | ((uint32_t)hi << 16);
     }
   }
-  if (lane == 0) scales[t] = s;
+  if (live && sl == 0) scales[t] = s;
 }
 
 // y = x - y (elementwise, n multiple of 4)
