@@ -733,7 +733,9 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
             "pct_hbm_peak": 100 * head["gbs"] / world / pk["hbm_gbs"],
             "forms": out, "max_rel_err_output_scaled_sample": head["max_rel_err_output_scaled_sample"],
             "speedup_vs_launch_loop": out["launch_loop"]["ms_per_step"] / head["ms_per_step"],
-            "clocks": head["clocks"], "gpu_launches": head["steps"]}))
+            "clocks": head["clocks"],
+            "gpu_launches": head["steps"] * (per_class if hname == "per_class" else batch).launch_count(),
+            "gpu_launches_note": "launches in one timed block of `steps` steps (the value is the median block)"}))
 
 
 def run_shapes(args, rank, local, torch):

@@ -80,6 +80,7 @@ EXTRA_SIGNATURES = [
     ("bridct_ragged_timeout_flag", C.c_int, [C.c_void_p]),
     ("bridct_ragged_set_wait_limit", C.c_int, [C.c_void_p, C.c_uint]),
     ("bridct_ragged_class_count", C.c_size_t, [C.c_void_p]),
+    ("bridct_ragged_launch_count", C.c_size_t, [C.c_void_p]),
     ("bridct_ragged_class_info", C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                            C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_int)]),
     ("bridct_ragged_set_schedule", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_size_t, C.c_int]),

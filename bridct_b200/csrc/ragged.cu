@@ -454,6 +454,15 @@ BRIDCT_API int bridct_ragged_apply_device(bridct_ragged* r, const float* x, floa
 
 BRIDCT_API size_t bridct_ragged_class_count(const bridct_ragged* r) { return r ? r->classes.size() : 0; }
 
+BRIDCT_API size_t bridct_ragged_launch_count(const bridct_ragged* r) {
+  if (!r) return 0;
+  size_t n = r->merged.size() + (r->units.empty() ? 0 : 1);
+  for (const RaggedClass& c : r->classes)
+    if (c.schedule == BRIDCT_RAGGED_CLASS_LAUNCH || c.schedule == BRIDCT_RAGGED_CLASS_LAUNCH_SMALL)
+      n += c.h * c.w <= 16384 || whole_array_route(c.h, c.w, c.mode) ? 1 : 2;
+  return n;
+}
+
 BRIDCT_API int bridct_ragged_class_info(const bridct_ragged* r, size_t cls, int* height, int* width, int* mode,
                                         size_t* arrays, int* schedule) {
   if (!r || cls >= r->classes.size()) return BRIDCT_INVALID_ARGUMENT;

@@ -84,6 +84,10 @@ class RaggedBatch:
     def units(self) -> int:
         return int(_lib.lib().bridct_ragged_units(self._h))
 
+    def launch_count(self) -> int:
+        """Kernel launches of one apply with the current schedule."""
+        return int(_lib.lib().bridct_ragged_launch_count(self._h))
+
     def classes(self) -> List[dict]:
         """Shape classes, largest first: {"key": "HxW/mode", "h", "w", "mode", "arrays", "schedule"}."""
         import ctypes as C

@@ -166,6 +166,10 @@ enum bridct_ragged_schedule {
                                               (row length, mode) over all MERGED classes      */
 };
 BRIDCT_API size_t bridct_ragged_class_count(const bridct_ragged *batch);
+/* Kernel launches of one bridct_ragged_apply_device call with the current schedule: the merged
+ * passes, one or two per class with its own launches, and the persistent queue kernel when any
+ * class is queued. */
+BRIDCT_API size_t bridct_ragged_launch_count(const bridct_ragged *batch);
 /* Shape, mode, array count and schedule of class `cls` (any output pointer may be NULL). */
 BRIDCT_API int bridct_ragged_class_info(const bridct_ragged *batch, size_t cls, int *height, int *width,
                                         int *mode, size_t *arrays, int *schedule);

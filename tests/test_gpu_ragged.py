@@ -284,3 +284,33 @@ def test_merged_schedule_rejects_single_pass_classes():
     arr = (C.c_int * len(cls))(*[3 if c["h"] * c["w"] <= 16384 else 0 for c in cls])
     assert _lib.lib().bridct_ragged_set_schedule(b._h, arr, len(cls), 2) == _lib.INVALID_ARGUMENT
     assert "two-pass" in _lib.last_error()
+
+
+def test_launch_count_matches_the_kernels_one_apply_runs():
+    """bridct_ragged_launch_count (the figure bench.py reports as gpu_launches) against the
+    kernels the CUDA profiler records for one apply: the queue alone, then a mixed schedule."""
+    from torch.profiler import ProfilerActivity, profile
+
+    from bridct_b200.ragged import two_pass
+
+    items = random_batch(120, 31) + [(1024, 1024, 0), (512, 256, 1), (64, 64, 0), (1024, 32, 1)]
+    b = RaggedBatch(items)
+    x = torch.from_numpy(np.random.default_rng(32).uniform(-1, 1, b.span).astype(np.float32)).cuda()
+    sched = {}
+    for i, c in enumerate(b.classes()):
+        if two_pass(c["h"], c["w"], c["mode"]) and i % 2:
+            sched[c["key"]] = "merged"
+        else:
+            sched[c["key"]] = ("launch", "queue", "launch_small" if c["h"] * c["w"] > 16384 else "launch")[i % 3]
+    m = RaggedBatch(items, schedule={"classes": sched, "streams": 4})
+    assert b.launch_count() == 1
+    for batch in (b, m):
+        y = batch.apply(x)
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            batch.apply(x, y)
+            torch.cuda.synchronize()
+        kernels = [e for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA
+                   and "memset" not in e.name.lower() and "memcpy" not in e.name.lower()]
+        assert len(kernels) == batch.launch_count(), sorted(e.name for e in kernels)
+    assert m.launch_count() > 1
