@@ -627,6 +627,29 @@ def main():
     print(json.dumps(line))
 
 
+def ragged_share(wl, rank: int, world: int):
+    """Rank's share of a job made of `world` copies of the ragged workload: the contiguous run of
+    arrays that bridct_b200.dist.ragged_shard_range gives it (balanced by elements) and the
+    matching slice of the job's packed input, built from the copies it spans."""
+    from bridct_b200.dist import ragged_shard_range
+
+    items = list(wl["items"]) * world
+    sizes = [h * w for h, w, _ in items]
+    first, count = ragged_shard_range(sizes, rank, world)
+    start = sum(sizes[:first])
+    end = start + sum(sizes[first:first + count])
+    span = sum(sizes[:len(wl["items"])])
+    pieces, pos = [], start
+    while pos < end:
+        off = pos % span
+        take = min(end - pos, span - off)
+        pieces.append(wl["x"][off:off + take])
+        pos += take
+    x = np.concatenate(pieces) if pieces else np.zeros(0, np.float32)
+    return dict(wl, items=items[first:first + count], x=x,
+                desc=wl["desc"] + f"; rank {rank}: arrays {first}..{first + count - 1} of {world} copies")
+
+
 def run_ragged(args, wl, rank, world, local, dist, torch):
     """Mixed-shape batch: one persistent launch per step vs one launch per array."""
     from bridct_b200.dist import max_over_ranks
@@ -638,6 +661,9 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
         items = wl["items"][:args.batch]
         span = sum(h * w for h, w, _ in items)
         wl = dict(wl, items=items, x=wl["x"][:span], desc=wl["desc"] + f"; first {len(items)} arrays")
+    job_bytes = 8.0 * sum(h * w for h, w, _ in wl["items"]) * world
+    if world > 1:   # the job is `world` copies of the batch, cut by elements (balanced h * w)
+        wl = ragged_share(wl, rank, world)
     x = torch.from_numpy(wl["x"]).to(dev)
     tuning = None
     class_schedule = None
@@ -662,7 +688,6 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
     per_class = RaggedBatch(wl["items"], tuning=tuning, schedule=class_schedule) if class_schedule else None
     y = torch.empty_like(x)
     stream = torch.cuda.Stream(device=dev)
-    bytes_step = 8.0 * batch.span
     out = {}
     legs = [("persistent", batch.apply)]
     if per_class is not None:
@@ -694,7 +719,7 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
         with clk:
             blocks = time_blocks(torch, stream, replay, nblocks, dev)
         ms = statistics.median(blocks) / args.steps
-        out[name] = {"ms_per_step": ms, "gbs": bytes_step * world / (ms * 1e-3) / 1e9, "clocks": clk.summary(),
+        out[name] = {"ms_per_step": ms, "gbs": job_bytes / (ms * 1e-3) / 1e9, "clocks": clk.summary(),
                      "steps": args.steps, "spread": spread(blocks)}
         del g
         # accuracy of this leg's output on a sample of arrays, against float64
@@ -726,8 +751,9 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
             "config": {"workload": wl["desc"], "arrays": len(wl["items"]), "floats": batch.span,
                        "units": batch.units, "tuning": tuning or "default", "form": hname,
                        "class_schedule": sched,
-                       "parallelism": "single GPU" if world == 1 else f"dp{world}: every rank its own copy "
-                       "of the batch (no collective)",
+                       "parallelism": "single GPU" if world == 1 else f"dp{world}: a job of {world} copies of "
+                       "the batch cut into contiguous runs of arrays balanced by elements (h * w), one per rank "
+                       "(no collective on the data; timing is the max over ranks)",
                        "timing": f"median of {head['spread']['blocks']} blocks of {args.steps} steps "
                                  "(CUDA-graph replays), CUDA events on the launch stream; inputs 1 GB > L2"},
             "pct_hbm_peak": 100 * head["gbs"] / world / pk["hbm_gbs"],

@@ -9,6 +9,12 @@ device-measured duration).
     mine, first = shard(x, rank, world)                 # the slice itself (a view)
     y = apply_sharded(x, mode, devices=[0, 1, 2, 3])    # one process driving several GPUs
     full = gather_shards(y_mine, first, batch)          # tests / callers that want one array back
+
+A ragged batch (arrays of mixed shapes packed back to back) shards by elements instead of by
+arrays, so that ranks get equal work whatever the mix:
+
+    first, count = ragged_shard_range([h * w for h, w, _ in items], rank, world)
+    my_items, x_mine, first = ragged_shard(items, x_packed, rank, world)   # a slice of the buffer
 """
 from __future__ import annotations
 
@@ -22,6 +28,41 @@ def shard_range(batch: int, rank: int, world: int) -> Tuple[int, int]:
     base, extra = divmod(batch, world)
     first = rank * base + min(rank, extra)
     return first, base + (1 if rank < extra else 0)
+
+
+def ragged_shard_range(sizes: Sequence[int], rank: int, world: int) -> Tuple[int, int]:
+    """(first, count) of rank's contiguous run of a ragged batch's arrays, balanced by elements.
+
+    sizes[i] is array i's element count (h * w).  With the arrays packed back to back in T
+    elements, rank r takes the arrays whose first element lies in [r T / world, (r + 1) T / world):
+    every rank's share is within one array of T / world elements, and its arrays are one
+    contiguous slice of the packed buffer (no gather)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("invalid rank/world")
+    if any(int(s) < 0 for s in sizes):
+        raise ValueError("negative array size")
+    total = sum(int(s) for s in sizes)
+    first = count = 0
+    pos = 0
+    for i, s in enumerate(sizes):
+        owner = pos * world // total if total else 0
+        if owner < rank:
+            first = i + 1
+        elif owner == rank:
+            count += 1
+        pos += int(s)
+    return first, count
+
+
+def ragged_shard(items: Sequence[Tuple[int, int, int]], x, rank: int, world: int):
+    """Rank's share of a ragged batch packed back to back in x (a flat numpy array or tensor):
+    (its items, the slice of x that holds them, index of its first item).  The slice is a view,
+    itself packed back to back, so it is the input of a RaggedBatch of those items."""
+    sizes = [h * w for h, w, _ in items]
+    first, count = ragged_shard_range(sizes, rank, world)
+    start = sum(sizes[:first])
+    end = start + sum(sizes[first:first + count])
+    return list(items[first:first + count]), x[start:end], first
 
 
 def shard(x, rank: int, world: int):

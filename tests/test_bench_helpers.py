@@ -42,3 +42,18 @@ def test_block_count_and_spread():
 def test_parallelism_text():
     assert bench.parallelism(1, 262144, 0) == "single GPU"
     assert "dp4" in bench.parallelism(4, 262144, 262144) and "no collective" in bench.parallelism(4, 1, 1)
+
+
+def test_ragged_share_cuts_n_copies_by_elements():
+    rng = np.random.default_rng(7)
+    items = [(int(2 ** rng.integers(3, 8)), int(2 ** rng.integers(3, 8)), int(rng.integers(0, 2)))
+             for _ in range(60)]
+    span = sum(h * w for h, w, _ in items)
+    wl = {"items": items, "x": np.arange(span, dtype=np.float32), "desc": "mix"}
+    for world in (2, 3, 5):
+        shares = [bench.ragged_share(wl, r, world) for r in range(world)]
+        assert sum((s["items"] for s in shares), []) == items * world          # contiguous runs, in order
+        assert np.array_equal(np.concatenate([s["x"] for s in shares]), np.tile(wl["x"], world))
+        for s in shares:
+            assert s["x"].size == sum(h * w for h, w, _ in s["items"])
+            assert abs(s["x"].size - span) <= max(h * w for h, w, _ in items)  # within one array of equal

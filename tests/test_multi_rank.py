@@ -1,10 +1,12 @@
 """Host-side multi-rank logic on CPU: two gloo ranks partition a batch with no overlap and no
 data collective, agree on the max-over-ranks timing, and, transforming their own shards (with the
 oracle standing in for each rank's GPU), stitch back exactly the full-batch result.  The same
-partition (bridct_b200.dist.shard / shard_range) feeds bench.py --gpus N and apply_sharded."""
+partition (bridct_b200.dist.shard / shard_range) feeds bench.py --gpus N and apply_sharded; ragged
+batches split by elements (ragged_shard_range), as bench.py --workload ragged --gpus N does."""
 import os
 import socket
 
+import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
@@ -125,3 +127,73 @@ def test_apply_sharded_partition_logic_on_cpu():
         stitch([(0, x[:3]), (4, x[4:])], 11)
     part, first = shard(x, 2, 3)
     assert first == 8 and part.shape[0] == 3
+
+
+def test_ragged_shard_range_balances_elements():
+    from bridct_b200.dist import ragged_shard_range
+
+    rng = np.random.default_rng(9)
+    sizes = [int(a * b) for a, b in zip(2 ** rng.integers(3, 11, 700), 2 ** rng.integers(3, 11, 700))]
+    total = sum(sizes)
+    for world in (1, 2, 3, 4, 8, 1000):
+        spans = [ragged_shard_range(sizes, r, world) for r in range(world)]
+        assert spans[0][0] == 0 and sum(c for _, c in spans) == len(sizes)
+        for (a, n), (b, _) in zip(spans, spans[1:]):
+            assert a + n == b                                                   # contiguous, in order
+        for f, c in spans:
+            assert abs(sum(sizes[f:f + c]) - total / world) <= max(sizes)       # within one array
+    assert ragged_shard_range([], 0, 2) == (0, 0)
+    with pytest.raises(ValueError):
+        ragged_shard_range([64], 2, 2)
+
+
+def _ragged_worker(rank, world, port, q):
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+
+    from bridct_b200.dist import ragged_shard
+    from oracle import oracle as O
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        rng = np.random.default_rng(12)
+        items = [(int(2 ** rng.integers(3, 7)), int(2 ** rng.integers(3, 7)), int(rng.integers(0, 3)))
+                 for _ in range(41)]
+        x = rng.uniform(-1, 1, sum(h * w for h, w, _ in items)).astype(np.float32)
+        mine, xs, first = ragged_shard(items, x, rank, world)     # a slice of the packed buffer
+        out, pos = [], 0
+        for h, w, m in mine:                                       # the oracle stands in for the GPU
+            out.append(O.sj_apply(xs[pos:pos + h * w].reshape(1, h, w), m).ravel())
+            pos += h * w
+        y_mine = np.concatenate(out) if out else np.zeros(0, np.float32)
+        parts = [None] * world
+        dist.all_gather_object(parts, (first, len(mine), y_mine))
+        if rank == 0:
+            whole, pos = [], 0
+            for h, w, m in items:
+                whole.append(O.sj_apply(x[pos:pos + h * w].reshape(1, h, w), m).ravel())
+                pos += h * w
+            got = np.concatenate([p[2] for p in sorted(parts, key=lambda p: p[0])])
+            q.put(("ok", bool(np.array_equal(got, np.concatenate(whole))), [p[1] for p in parts]))
+    except Exception as e:  # pragma: no cover - reported to the parent
+        q.put(("error", repr(e), []))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_transform_balanced_ragged_shards():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_ragged_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    status, same, counts = q.get(timeout=10)
+    assert status == "ok" and same, (status, same)
+    assert sum(counts) == 41 and min(counts) > 0
