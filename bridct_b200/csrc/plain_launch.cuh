@@ -6,6 +6,24 @@
 
 namespace bridct {
 
+// Tile-class batches of at most this many floats (16 MiB) take the small-batch tiles where
+// small_batch_tiles says so.
+constexpr long long kSmallBatchFloats = 4LL << 20;
+
+// Shapes and modes whose 16 MiB batches measured faster with tiles of half the 8192-float target
+// (several CTAs per SM instead of one uneven wave of large tiles; 24 shapes A/B'd on one box):
+// 8x16 +17%, 16x16 +16%, 32x16 +9..12%, 16x64 +8..14%, 32x32 +8..10%, 16x32 +6..10%, 8x32 +4..10%,
+// 16x8 +5%, 64x8 +4..7%, and the inverse and round trip of 32x64 (+10..13%) and the round trip of
+// 8x64 (+9%).  Tiles of 64-point register lines (64x16, 64x32, 64x64: one thread per line, so a
+// 4096-float tile leaves most threads idle) and of 128-point lines measured 5..25% slower.  64x64
+// round trips instead take two arrays per 128-thread CTA (a thread for each register line): +11%;
+// forward equal, inverse 5% slower that way.
+__host__ __device__ constexpr bool small_batch_tiles(int h, int w, int mode) {
+  return (h == 8 && (w == 16 || w == 32)) || (h == 16 && w <= 64) || (h == 32 && (w == 16 || w == 32)) ||
+         (h == 64 && w == 8) || (h == 32 && w == 64 && mode != LM_FWD) || (h == 8 && w == 64 && mode == LM_RT) ||
+         (h == 64 && w == 64 && mode == LM_RT);
+}
+
 struct LaunchCtx {
   int sm_count;
 };
@@ -117,6 +135,17 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     // round trips +3..30% together with their register lines).  Forward / inverse tiles that mix
     // 128-point register lines with many short lines measured 5..13% slower that way.
     constexpr int T = (H == 128 && W == 128) || (MODE == LM_RT && (H == 128 || W == 128)) ? 128 : kThreads;
+    if constexpr (Gm::kTRSmall < TR && small_batch_tiles(H, W, MODE)) {
+      if (batch * H * W <= kSmallBatchFloats) {
+        constexpr bool k64 = H == 64 && W == 64;   // two arrays, 128 threads (see small_batch_tiles)
+        constexpr int TS = k64 ? 128 : T;
+        constexpr int TRS = k64 ? Gm::kTR : Gm::kTRSmall;
+        constexpr int SMS = k64 ? Gm::kSmemFull : Gm::kSmemFullSmall;
+        auto ks = k_full<H, W, TRS, true, true, MODE, TS, GEN>;
+        TileArgs a{x, y, (batch * H + TRS - 1) / TRS, batch * H, tab, lx, ly};
+        return launch_tiles(ks, SMS, kernel_blocks_per_sm(ks, SMS, TS), a, ctx, st, TS);
+      }
+    }
     auto k = k_full<H, W, TR, true, true, MODE, T, GEN>;
     const int bps = kernel_blocks_per_sm(k, smem, T);
     TileArgs a{x, y, (batch * H + TR - 1) / TR, batch * H, tab, lx, ly};

@@ -536,6 +536,11 @@ struct Geometry {
   static constexpr int kArraysBig = pick_arrays(2 * kTileFloats);
   static constexpr int kTRBig = kTile ? kArraysBig * H : 1;
   static constexpr int kSmemFullBig = full_smem(kArraysBig);
+  // Tiles of a quarter of the target for small batches, so that a batch of a few MiB spreads over
+  // several CTAs per SM instead of one uneven wave (see launch_plain).
+  static constexpr int kArraysSmall = pick_arrays(kTileFloats / 2);
+  static constexpr int kTRSmall = kTile ? kArraysSmall * H : 1;
+  static constexpr int kSmemFullSmall = full_smem(kArraysSmall);
   // One whole array of 32768 floats per tile (one CTA per SM, 178-184 KB of shared memory), for
   // the two-pass shapes and modes where it measured faster than the two passes (launch_plain).
   static constexpr int kSmemWhole = full_smem(1);
