@@ -114,7 +114,10 @@ struct Fp8Layout {
   static constexpr int kTmemAlloc = kSets * UKT * 64 <= 256 ? 256 : 512;
   static constexpr int kStages = (196608 - kBBytes) / kStageBytes < 8 ? (196608 - kBBytes) / kStageBytes : 8;
   static constexpr int kBOff = kStages * kStageBytes;
-  static constexpr int kScOff = kBOff + kBBytes;       // sC of this CTA's two column bands
+  // rows shorter than 64 points: each epilogue warp's 64 x 32 outputs, staged for the stores
+  static constexpr int kStoreOff = kBOff + kBBytes;
+  static constexpr int kStoreBytes = L < 64 ? 4 * 64 * 33 * 4 : 0;
+  static constexpr int kScOff = kStoreOff + kStoreBytes;   // sC of this CTA's two column bands
   static constexpr int kBarOff = kScOff + 2 * kKT * 4 + 64;
   static constexpr int kDynamic = ((kBarOff + 255) / 256) * 256 + 256 + 1024;
   static_assert(LS % 128 == 0 && kKT % UKT == 0 && UKT % 4 == 0, "FP8 pass geometry");
@@ -153,6 +156,7 @@ __global__ void __launch_bounds__(256, 1)
                  acc_free = acc_full + 16;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + F::kBarOff + 16 * F::kStages + 32);
   float* s_sc = reinterpret_cast<float*>(base + F::kScOff);
+  float* s_store = reinterpret_cast<float*>(base + F::kStoreOff);
   __shared__ volatile int s_abort;
   __shared__ volatile int s_ok;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -295,14 +299,34 @@ __global__ void __launch_bounds__(256, 1)
 #pragma unroll
             for (int c = 0; c < 64; ++c) dst[(long long)c << rshift] = v[c];
           }
-        } else {
+        } else if constexpr (L == 64) {
 #pragma unroll
           for (int c = 0; c < 64; ++c) {
-            const int n = nblk * 64 + c;
-            const long long g = gs * SUB + n / L;
+            const long long g = gs * SUB + nblk;
             if (g < nrows) {
               const long long b = g >> rshift, h = g & rmask;
-              out[((b * L + n % L) << rshift) + h] = v[c];
+              out[((b * L + c) << rshift) + h] = v[c];
+            }
+          }
+        } else {
+          // The CTA's 64 columns are RUN = 64 / L whole sub-rows s0 + s of each super-row, so
+          // rows g = gs * SUB + s0 + s of one output column k come in runs of RUN consecutive
+          // rows: the warp stages its 32 super-rows x 64 columns (column-major, pitch 33) and
+          // stores element e = (k * 32 + lane_src) * RUN + s, a run of RUN floats per super-row.
+          constexpr int RUN = 64 / L;
+          float* wb = s_store + (warp & 3) * (64 * 33);
+          __syncwarp();
+#pragma unroll
+          for (int c = 0; c < 64; ++c) wb[c * 33 + lane] = v[c];
+          __syncwarp();
+          const long long gs0 = gs - lane;
+#pragma unroll 8
+          for (int e = lane; e < 64 * 32; e += 32) {
+            const int s = e % RUN, src = (e / RUN) % 32, k = e / (RUN * 32);
+            const long long g = (gs0 + src) * SUB + nblk * RUN + s;
+            if (g < nrows) {
+              const long long b = g >> rshift, h = g & rmask;
+              out[((b * L + k) << rshift) + h] = wb[(s * L + k) * 33 + src];
             }
           }
         }
