@@ -2,7 +2,7 @@
 tensor-core split-precision forms, with the reference's own CPU path timed on the host.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload blocks8|image8|arrays64|large1024|ragged|sweep256|shapes] [--form auto|sj|...]
+                    [--workload blocks8|image8|arrays64|large1024|ragged|ragged256|sweep256|shapes] [--form auto|sj|...]
 
 Default workload: 262,144 independent 8x8 blocks of a 4096x4096 image (pixels uniform integers
 0..255 minus 128, seed 1), forward DCT-II, blocks stored contiguously as (B, 8, 8).  A step is
@@ -76,16 +76,21 @@ def workload(name: str):
         yy, xx = np.mgrid[0:1024, 0:1024]
         x = (rng.standard_normal((1024, 1024)) + np.sin(2 * np.pi * xx / 97) * np.cos(2 * np.pi * yy / 61))
         return dict(x=x.astype(np.float32)[None], mode=0, desc="one 1024x1024 N(0,1)+smooth (seed 2), forward")
-    if name == "ragged":
+    if name in ("ragged", "ragged256"):
+        # ragged: the mixed-batch configuration; ragged256: the same generator over the axes up to
+        # 256 (the 8x8..256x256 range of the batching target), 16384 arrays so that the input
+        # (0.46 GB) is larger than L2
+        big = name == "ragged"
         rng = np.random.default_rng(3)
-        sizes = np.array([8, 16, 32, 64, 128, 256, 512, 1024])
-        hs, ws = rng.choice(sizes, 4096), rng.choice(sizes, 4096)
-        modes = rng.integers(0, 2, 4096)
+        sizes = np.array([8, 16, 32, 64, 128, 256, 512, 1024] if big else [8, 16, 32, 64, 128, 256])
+        n = 4096 if big else 16384
+        hs, ws = rng.choice(sizes, n), rng.choice(sizes, n)
+        modes = rng.integers(0, 2, n)
         span = int((hs * ws).sum())
         x = rng.uniform(-1, 1, span).astype(np.float32)
         return dict(x=x, mode=None, items=list(zip(hs.tolist(), ws.tolist(), modes.tolist())),
-                    desc="4096 arrays, each axis uniform in {8..1024} (all 64 shapes), U[-1,1], "
-                         "50% forward / 50% inverse (seed 3), packed back to back")
+                    desc=(f"{n} arrays, each axis uniform in {{8..{sizes[-1]}}} (all {len(sizes) ** 2} shapes), "
+                          "U[-1,1], 50% forward / 50% inverse (seed 3), packed back to back"))
     if name == "sweep256":
         rng = np.random.default_rng(4)
         mag = 10.0 ** rng.uniform(-6, 6, (2048, 256, 256))
@@ -401,14 +406,14 @@ def main():
     ap.add_argument("--form", default="auto")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--autotune", action="store_true",
-                    help="ragged workload: measure the unit geometry first and record it (see --tuning-out)")
+                    help="ragged workloads: measure the unit geometry first and record it (see --tuning-out)")
     ap.add_argument("--tuning-out", default="", help="where --autotune writes its result "
-                    "(default profiles/ragged_tuning.json)")
+                    "(default profiles/<workload>_tuning.json)")
     ap.add_argument("--batch", type=int, default=0,
                     help="use the first N arrays of the workload (repeated cyclically when N is larger)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 20 if args.workload == "ragged" else 200
+        args.steps = 20 if args.workload.startswith("ragged") else 200
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus))
@@ -437,7 +442,7 @@ def main():
                                 device_id=torch.device("cuda", local))
     lib = _lib.lib()
     wl = workload(args.workload)
-    if args.workload == "ragged":
+    if args.workload.startswith("ragged"):
         return run_ragged(args, wl, rank, world, local, dist, torch)
     if args.workload == "image8":
         return run_image8(args, wl, rank, world, local, dist, torch)
@@ -667,7 +672,7 @@ def run_ragged(args, wl, rank, world, local, dist, torch):
     x = torch.from_numpy(wl["x"]).to(dev)
     tuning = None
     class_schedule = None
-    tfile = ROOT / "profiles" / "ragged_tuning.json"
+    tfile = ROOT / "profiles" / f"{args.workload}_tuning.json"
     if args.autotune:
         from bridct_b200.autotune import tune, tune_classes
 

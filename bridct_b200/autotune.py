@@ -128,9 +128,10 @@ def tune_classes(items, x, tuning: Optional[Dict[str, int]] = None, steps: int =
     launch, and for two-pass shapes with the few-array geometry; the fastest wins.  The chosen
     schedule is then timed on the whole batch for each side-stream count, next to the all-queue
     and all-launch schedules, a hybrid (whole-array classes in the queue, two-pass classes in
-    their own launches) and a merged schedule (two-pass classes in merged column and row passes),
-    and the fastest whole-batch schedule is returned (its output checked against the all-queue
-    result).  Returns {"schedule", "ms", "queue_ms", "launch_ms", "classes"}."""
+    their own launches), a merged schedule (two-pass classes in merged column and row passes) and
+    size thresholds (classes under 1, 4, 16 or 64 MB in the queue, the rest in their own or merged
+    launches), and the fastest whole-batch schedule is returned (its output checked against the
+    all-queue result).  Returns {"schedule", "ms", "queue_ms", "launch_ms", "classes"}."""
     import torch
 
     from .ragged import RaggedBatch
@@ -168,9 +169,21 @@ def tune_classes(items, x, tuning: Optional[Dict[str, int]] = None, steps: int =
         return "queue" if "launch_small" not in r["ms"] else every_launch[r["class"]]
 
     merged = {r["class"]: merged_choice(r) for r in rows}
+    candidates = [("per_class", chosen), ("all_launch", every_launch), ("hybrid", hybrid), ("merged", merged)]
+    # by size: classes of fewer than `thr` bytes share the persistent queue (one launch for all of
+    # them, where alone each would be a launch-latency-bound launch of its own), larger classes keep
+    # their own launches, or for two-pass shapes the merged passes
+    def class_bytes(r):
+        h, w, _ = (int(v) for v in r["class"].replace("/", "x").split("x"))
+        return 8 * h * w * r["arrays"]
+
+    for thr in (1 << 20, 4 << 20, 16 << 20, 64 << 20):
+        big = [r for r in rows if class_bytes(r) >= thr]
+        candidates.append((f"size{thr >> 20}MB", {r["class"]: every_launch[r["class"]] for r in big}))
+        candidates.append((f"size{thr >> 20}MB_merged", {r["class"]: (merged[r["class"]] if merged[r["class"]] == "merged"
+                                                                         else every_launch[r["class"]]) for r in big}))
     trials = []
-    for name, classes in (("per_class", chosen), ("all_launch", every_launch), ("hybrid", hybrid),
-                          ("merged", merged)):
+    for name, classes in candidates:
         for n in streams:
             trials.append((name, {"classes": classes, "streams": int(n)}))
     results = [("all_queue", {"classes": {}, "streams": 1}, _time_graph(lambda s: batch.apply(x, y, stream=s), x, steps))]
