@@ -223,3 +223,40 @@ def test_back_to_back_dependent_launches(shape):
     assert torch.equal(c, torch_api.apply(b, 0))
     tol = 8e-6 * float(x.abs().max())
     assert float((d - x).abs().max()) <= tol
+
+
+def test_batch_entry_points_reject_empty_null_and_bad_mode_without_writing():
+    """Zero arrays, NULL buffers, a bad mode or an unknown form are INVALID_ARGUMENT on every batch
+    entry point (as NULL and bad modes are on the reference's plan API, src/plan.c:129-131), and
+    nothing is launched or written."""
+    from bridct_b200 import torch_api
+
+    L = _lib.lib()
+    INV = _lib.INVALID_ARGUMENT
+    p = torch_api._plan(torch.cuda.current_device(), 16, 32)
+    x = torch.randn(2, 16, 32, device="cuda")
+    y = torch.full_like(x, 7.0)
+    xp, yp = x.data_ptr(), y.data_ptr()
+    assert L.bridct_plan_apply_device(p, 0, xp, yp, 0, None) == INV
+    assert L.bridct_plan_apply_device(p, 0, None, yp, 2, None) == INV
+    assert L.bridct_plan_apply_device(p, 0, xp, None, 2, None) == INV
+    for form in (_lib.FORM_TC_BF16X3, _lib.FORM_TC_TF32X3, _lib.FORM_TC_FP8):
+        assert L.bridct_plan_apply_form_device(p, 0, form, xp, yp, 0, None) == INV
+        assert L.bridct_plan_apply_form_device(p, 3, form, xp, yp, 2, None) == INV
+        assert L.bridct_plan_apply_form_device(p, 0, form, None, yp, 2, None) == INV
+        assert L.bridct_plan_form_workspace_bytes(p, form, 0) == 0
+    assert L.bridct_plan_apply_form_device(p, 0, 9, xp, yp, 2, None) == INV
+    assert L.bridct_plan_apply_strided_device(p, 0, xp, 32, 512, yp, 32, 512, 0, None) == INV
+    assert L.bridct_plan_apply_strided_device(p, 3, xp, 32, 512, yp, 32, 512, 2, None) == INV
+    xh = np.ones((2, 16, 32), np.float32)
+    yh = np.full_like(xh, 7.0)
+    assert L.bridct_plan_apply_batch(p, 0, xh.ctypes.data, yh.ctypes.data, 0) == INV
+    assert L.bridct_plan_apply_batch(p, 3, xh.ctypes.data, yh.ctypes.data, 2) == INV
+    assert L.bridct_plan_roundtrip_batch(p, xh.ctypes.data, yh.ctypes.data, 0) == INV
+    assert L.bridct_plan_roundtrip_batch(p, None, yh.ctypes.data, 2) == INV
+    items = (_lib.RaggedItem * 1)(_lib.RaggedItem(16, 32, 0, 0, 0))
+    assert not L.bridct_ragged_create(items, 0)
+    assert not L.bridct_ragged_create(None, 1)
+    assert L.bridct_ragged_apply_noalloc(items, 0, xp, yp, None) == INV
+    torch.cuda.synchronize()
+    assert (y == 7.0).all() and (yh == 7.0).all()

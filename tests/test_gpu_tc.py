@@ -299,3 +299,17 @@ def test_tc_golden_config_samples(form):
             y = run(x, mode, form)
             ref = g[k[:-2] + f"_y{mode}"]
             assert O.rel_max_error(y, ref, x, output_scaled=True) <= 2 * sep_tol(form, mode), (k, mode)
+
+
+@pytest.mark.parametrize("shape", [(8, 8), (8, 1024), (1024, 16), (32, 512), (16, 64)])
+def test_fp8_per_array_magnitudes(shape):
+    """Arrays of magnitudes 1e-6..1e6 side by side (arrays of short rows share super-rows): every
+    array meets the FP8 bound on its own scale, since scale tiles never span two arrays."""
+    rng = np.random.default_rng(shape[0] * 7 + shape[1])
+    mag = 10.0 ** rng.uniform(-6, 6, (33, 1, 1))
+    x = (mag * rng.uniform(-1, 1, (33, *shape))).astype(np.float32)
+    for mode in range(2):
+        y = run(x, mode, "tc_fp8")
+        ref = O.fp64_apply(x, mode)
+        for i in range(x.shape[0]):
+            assert O.rel_max_error(y[i:i + 1], ref[i:i + 1], x[i:i + 1], output_scaled=True) <= FP8_MAX, (shape, mode, i)
