@@ -126,6 +126,23 @@ __host__ __device__ constexpr int strip_pitch(int h, int tc) {
   return h == 256 || (h == 512 && tc == 32) ? tc + 2 : pitch_of(h, tc, true);
 }
 __host__ __device__ constexpr int rowblock_pitch(int w) { return w == 256 ? w + 8 : w == 512 ? w + 16 : w + 4; }
+// Array pitch in a whole-array tile.  With pitch w + 4, h * (w + 4) is a multiple of 32 floats for
+// every shape, so the register-line column walks of the 4 (w = 8) or 2 (w = 16) arrays that a
+// warp's 32 lines span share banks (4- and 2-way conflicts; the tile kernel of 32 x 8 arrays spent
+// most of its time in mio_throttle stalls).  Arrays of 8 columns up to 128 high and of 16 columns
+// up to 64 high are padded to 8 and 16 (mod 32) floats apart instead: 16..64 x 8 +16..26%,
+// 128 x 8 +8..12%, 8..32 x 16 +5..11%, 64 x 16 +4% (same-box A/B, all modes).  128 x 16 (-5%
+// forward) and the taller four-step shapes (-1..2%) keep the plain layout.
+__host__ __device__ constexpr int tile_array_pitch(int h, int w, int p) {
+  return w == 8 && h <= 128 ? h * p + (40 - (h * p) % 32) % 32
+                            : w == 16 && h <= 64 ? h * p + (48 - (h * p) % 32) % 32 : h * p;
+}
+// Shared-memory offset of row r of a tile whose rows come in groups of AH (one array each), AP
+// floats apart, and P floats apart within a group (AH = 1, AP = P: every row P apart).
+template <int P, int AH, int AP>
+__device__ __forceinline__ int tile_row(int r) {
+  return AH == 1 ? r * AP : (r / AH) * AP + (r % AH) * P;
+}
 
 // Asynchronous global -> shared copies (cp.async; 16 bytes through L2 only, 8 and 4 bytes through
 // L1).  The issuing thread waits with cp_async_wait_all; a barrier then publishes the data.
@@ -149,13 +166,13 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // on tiles of short lines and +6..12% on 1024-point row passes.  An odd pitch (column passes of
 // 512- and 1024-point lines) would need four 4-byte copies per float4, which measured 6-14% slower
 // than the synchronous float4 load it keeps.
-template <int P>
+template <int P, int AH = 1, int AP = P>
 __device__ __forceinline__ void tile_load(const float* g, long long gp, int rows, int cols, float* tile,
                                           int valid_rows) {
   const int q = cols / 4;
   for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
     const int r = i / q, c = (i % q) * 4;
-    float* d = tile + r * P + c;
+    float* d = tile + tile_row<P, AH, AP>(r) + c;
     if constexpr (P % 2 == 0) {
       if (r < valid_rows) {
         const float* src = g + r * gp + c;
@@ -181,7 +198,7 @@ __device__ __forceinline__ void tile_load(const float* g, long long gp, int rows
 // next tile's loads are in flight while the current tile is transformed (ROWS x COLS floats,
 // row pitch P in shared memory; element i of the tile's float4 sequence goes to thread
 // i % THREADS).
-template <int P, int ROWS, int COLS, int THREADS = kThreads>
+template <int P, int ROWS, int COLS, int THREADS = kThreads, int AH = 1, int AP = P>
 struct TileRegs {
   static constexpr int Q = COLS / 4;
   static constexpr int N = (ROWS * Q + THREADS - 1) / THREADS;
@@ -216,7 +233,7 @@ struct TileRegs {
       const int i = threadIdx.x + k * THREADS;
       if (ROWS * Q % THREADS == 0 || i < ROWS * Q) {
         const int r = i / Q, c = (i % Q) * 4;
-        float* d = tile + r * P + c;
+        float* d = tile + tile_row<P, AH, AP>(r) + c;
         if constexpr (P % 4 == 0) {
           *reinterpret_cast<float4*>(d) = v[k];
         } else if constexpr (P % 2 == 0) {
@@ -231,12 +248,12 @@ struct TileRegs {
 };
 
 // tile_load for tiles whose rows lie anywhere (row r at rp(r), 16-byte aligned).
-template <int P, typename RowPtr>
+template <int P, int AH = 1, int AP = P, typename RowPtr>
 __device__ __forceinline__ void tile_load_rows(const RowPtr& rp, int rows, int cols, float* tile, int valid_rows) {
   const int q = cols / 4;
   for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
     const int r = i / q, c = (i % q) * 4;
-    float* d = tile + r * P + c;
+    float* d = tile + tile_row<P, AH, AP>(r) + c;
     if constexpr (P % 2 == 0) {
       if (r < valid_rows) {
         const float* src = rp(r) + c;
@@ -259,12 +276,12 @@ __device__ __forceinline__ void tile_load_rows(const RowPtr& rp, int rows, int c
 }
 
 // tile_store for tiles whose rows lie anywhere; rows from valid_rows on are not stored.
-template <int P, typename RowPtr>
+template <int P, int AH = 1, int AP = P, typename RowPtr>
 __device__ __forceinline__ void tile_store_rows(const RowPtr& rp, int rows, int cols, const float* tile) {
   const int q = cols / 4;
   for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
     const int r = i / q, c = (i % q) * 4;
-    const float* sp = tile + r * P + c;
+    const float* sp = tile + tile_row<P, AH, AP>(r) + c;
     float4 v;
     if constexpr (P % 4 == 0) {
       v = *reinterpret_cast<const float4*>(sp);
@@ -278,12 +295,12 @@ __device__ __forceinline__ void tile_store_rows(const RowPtr& rp, int rows, int 
   }
 }
 
-template <int P>
+template <int P, int AH = 1, int AP = P>
 __device__ __forceinline__ void tile_store(float* g, long long gp, int rows, int cols, const float* tile) {
   const int q = cols / 4;
   for (int i = threadIdx.x; i < rows * q; i += blockDim.x) {
     const int r = i / q, c = (i % q) * 4;
-    const float* sp = tile + r * P + c;
+    const float* sp = tile + tile_row<P, AH, AP>(r) + c;
     float4 v;
     if constexpr (P % 4 == 0) {
       v = *reinterpret_cast<const float4*>(sp);
@@ -325,10 +342,13 @@ template <int H, int W, int TR, bool DO_COL, bool DO_ROW, int MODE, int THREADS 
 __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
   static_assert(!UNITS || !DO_COL, "merged units are row blocks");
   constexpr int P = DO_COL ? pitch_of(H, W, true) : rowblock_pitch(W);
+  // whole-array tiles: arrays of H rows, AP floats apart (tile_array_pitch); row blocks: rows P apart
+  constexpr int AH = DO_COL ? H : 1;
+  constexpr int AP = DO_COL ? tile_array_pitch(H, W, P) : P;
   constexpr int XB = (THREADS / 32) * cmax(DO_COL ? ExchangeFloats<H>::value : 0, DO_ROW ? ExchangeFloats<W>::value : 0);
   extern __shared__ float smem[];
   float* tile = smem;
-  float* xbuf = smem + round4(TR * P);
+  float* xbuf = smem + round4((TR / AH) * AP);
   float* tabs = xbuf + round4(XB);
   griddep_wait();
   const FourStepTables tcol = DO_COL ? stage_tables<H>(a.tab.col, tabs) : a.tab.col;
@@ -361,7 +381,7 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
     };
   };
   constexpr bool kRows = GEN || UNITS;   // per-row addressing
-  TileRegs<P, kPrefetch ? TR : 4, kPrefetch ? W : 4, THREADS> next;
+  TileRegs<P, kPrefetch ? TR : 4, kPrefetch ? W : 4, THREADS, AH, AP> next;
   if (kPrefetch && blockIdx.x < a.ntiles) {
     if constexpr (kRows) next.load_rows(xrow(blockIdx.x), rows_of(blockIdx.x));
     else next.load(a.x + blockIdx.x * (long long)TR * W, W, rows_of(blockIdx.x));
@@ -377,14 +397,14 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
         else next.load(a.x + (t + gridDim.x) * (long long)TR * W, W, rows_of(t + gridDim.x));
       }
     } else {
-      if constexpr (kRows) tile_load_rows<P>(xrow(t), TR, W, tile, rows);
-      else tile_load<P>(a.x + t * (long long)TR * W, W, TR, W, tile, rows);
+      if constexpr (kRows) tile_load_rows<P, AH, AP>(xrow(t), TR, W, tile, rows);
+      else tile_load<P, AH, AP>(a.x + t * (long long)TR * W, W, TR, W, tile, rows);
       __syncthreads();
     }
     if constexpr (DO_COL) {
       static_assert(TR % H == 0, "column pass needs whole arrays");
       run_lines<H, MODE, reg_line_max(H, W, MODE, false)>(tile, (TR / H) * W, P,
-                         [](int l) { return (l / W) * H * P + (l % W); }, xbuf, tcol);
+                         [](int l) { return (l / W) * AP + (l % W); }, xbuf, tcol);
       __syncthreads();
     }
     if constexpr (DO_ROW) {
@@ -392,11 +412,11 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
       // conflicts there, while 256-point rows (no fewer wavefronts at their pitch, plus the
       // shuffles) measured 7-12% slower with them.
       run_lines<W, MODE, reg_line_max(W, H, MODE, !DO_COL), P % 2 == 0 && W >= 512>(
-          tile, TR, 1, [](int l) { return l * P; }, xbuf, trow);
+          tile, TR, 1, [](int l) { return tile_row<P, AH, AP>(l); }, xbuf, trow);
       __syncthreads();
     }
-    if constexpr (kRows) tile_store_rows<P>(yrow(t), rows, W, tile);
-    else tile_store<P>(a.y + t * (long long)TR * W, W, rows, W, tile);
+    if constexpr (kRows) tile_store_rows<P, AH, AP>(yrow(t), rows, W, tile);
+    else tile_store<P, AH, AP>(a.y + t * (long long)TR * W, W, rows, W, tile);
     __syncthreads();
   }
 }
@@ -522,7 +542,7 @@ struct Geometry {
   // tile class
   static constexpr int kXbufFull = kWarps * cmax(ExchangeFloats<H>::value, ExchangeFloats<W>::value);
   static constexpr int full_smem(int arrays) {
-    return (round4(arrays * H * pitch_of(H, W, true)) + round4(kXbufFull) + TableFloats<H>::value +
+    return (round4(arrays * tile_array_pitch(H, W, pitch_of(H, W, true))) + round4(kXbufFull) + TableFloats<H>::value +
             TableFloats<W>::value) * 4;
   }
   static constexpr int pick_arrays(int target) {

@@ -180,3 +180,24 @@ def test_transposed_512_point_strips():
     for pitch, tc in ((1028, 16), (1026, 8)):
         q = tc // 4
         assert max(wavefronts([(4 * (l % q) + j) * pitch + l // q for l in range(32)]) for j in range(4)) == 2
+
+
+def test_padded_arrays_make_narrow_tile_columns_conflict_free():
+    """Whole-array tiles of 8- and 16-column arrays (pitch w + 4): h * (w + 4) is a multiple of 32
+    floats, so a warp's 32 register-line column walks over 4 or 2 arrays share banks; padding the
+    arrays to 8 / 16 (mod 32) floats apart (tile_array_pitch in sj_kernels.cuh) removes it."""
+    def tile_array_pitch(h, w, p):
+        if w == 8 and h <= 128:
+            return h * p + (40 - (h * p) % 32) % 32
+        if w == 16 and h <= 64:
+            return h * p + (48 - (h * p) % 32) % 32
+        return h * p
+
+    for h, w in [(16, 8), (32, 8), (64, 8), (128, 8), (8, 16), (16, 16), (32, 16), (64, 16), (8, 8)]:
+        p = w + 4
+        ap = tile_array_pitch(h, w, p)
+        assert ap % 4 == 0                                    # rows stay 16-byte aligned
+        plain = sum(wavefronts([(l // w) * h * p + i * p + l % w for l in range(32)]) for i in range(h))
+        padded = sum(wavefronts([(l // w) * ap + i * p + l % w for l in range(32)]) for i in range(h))
+        assert padded == h, (h, w)
+        assert plain == h * 32 // w, (h, w)                  # 4-way (w = 8), 2-way (w = 16) before
