@@ -127,8 +127,13 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     // slower with them.
     constexpr bool kBig = (W == 64 && H <= 64 && !(H == 64 && MODE == LM_INV)) ||
                           (W == 128 && H <= 32 && MODE != LM_RT);
-    constexpr int TR = kBig ? Gm::kTRBig : Gm::kTR;
-    constexpr int smem = kBig ? Gm::kSmemFullBig : Gm::kSmemFull;
+    // Forward / inverse tiles of 128-point register columns and 8..32 columns hold one CTA per SM
+    // (227+ registers), so their tiles are sized against one CTA's shared memory (kTRWide): twice
+    // the arrays, so that 128 instead of 64 threads have a column line (+18..26%); round trips
+    // (128-thread CTAs, two per SM) measured 18-20% slower that way.
+    constexpr bool kWide = H == 128 && W <= 32 && MODE != LM_RT;
+    constexpr int TR = kWide ? Gm::kTRWide : kBig ? Gm::kTRBig : Gm::kTR;
+    constexpr int smem = kWide ? Gm::kSmemFullWide : kBig ? Gm::kSmemFullBig : Gm::kSmemFull;
     // 128 x 128 tiles (both passes 128-point register lines, 255 registers) and round trips of
     // tiles with a 128-point axis run 128-thread CTAs: two CTAs share an SM (128 x 128 +31..64%
     // over one 256-thread CTA with register prefetch, in which half the warps have no line; the

@@ -545,9 +545,9 @@ struct Geometry {
     return (round4(arrays * tile_array_pitch(H, W, pitch_of(H, W, true))) + round4(kXbufFull) + TableFloats<H>::value +
             TableFloats<W>::value) * 4;
   }
-  static constexpr int pick_arrays(int target) {
+  static constexpr int pick_arrays(int target, int cap = kSmemTwoPerSM) {
     int a = cmax(1, target / (H * W));
-    while (a > 1 && full_smem(a) > kSmemTwoPerSM) a /= 2;
+    while (a > 1 && full_smem(a) > cap) a /= 2;
     return a;
   }
   static constexpr int kArrays = pick_arrays(kTileFloats);
@@ -557,6 +557,11 @@ struct Geometry {
   static constexpr int kArraysBig = pick_arrays(2 * kTileFloats);
   static constexpr int kTRBig = kTile ? kArraysBig * H : 1;
   static constexpr int kSmemFullBig = full_smem(kArraysBig);
+  // Tiles of twice the target for kernels that hold one CTA per SM anyway (128-point register
+  // lines, 227 registers): sized against one CTA's shared memory instead of two.
+  static constexpr int kArraysWide = pick_arrays(2 * kTileFloats, 2 * kSmemTwoPerSM);
+  static constexpr int kTRWide = kTile ? kArraysWide * H : 1;
+  static constexpr int kSmemFullWide = full_smem(kArraysWide);
   // Tiles of a quarter of the target for small batches, so that a batch of a few MiB spreads over
   // several CTAs per SM instead of one uneven wave (see launch_plain).
   static constexpr int kArraysSmall = pick_arrays(kTileFloats / 2);
