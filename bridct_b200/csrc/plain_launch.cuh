@@ -130,7 +130,8 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     // Forward / inverse tiles of 128-point register columns and 8..32 columns hold one CTA per SM
     // (227+ registers), so their tiles are sized against one CTA's shared memory (kTRWide): twice
     // the arrays, so that 128 instead of 64 threads have a column line (+18..26%); round trips
-    // (128-thread CTAs, two per SM) measured 18-20% slower that way.
+    // (128-thread CTAs, two per SM) measured 18-20% slower that way, and so did 32768-float tiles
+    // of 8..32 x 128 (all rows busy, but no register prefetch at that size): -20%.
     constexpr bool kWide = H == 128 && W <= 32 && MODE != LM_RT;
     constexpr int TR = kWide ? Gm::kTRWide : kBig ? Gm::kTRBig : Gm::kTR;
     constexpr int smem = kWide ? Gm::kSmemFullWide : kBig ? Gm::kSmemFullBig : Gm::kSmemFull;
