@@ -124,7 +124,8 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     // 16384-float tiles instead of 8192 where they measured faster on 128 MiB batches: 64-wide
     // arrays up to 64 high (+6..14%, except the 64 x 64 inverse, -2%) and forward/inverse of
     // 8..32 x 128 (+17..22%); narrower tiles, 64 x 128 and those round trips measured 5..21%
-    // slower with them.
+    // slower with them (64 x 8 and 64 x 16, whose 8192-float tiles give half the threads a column
+    // line, 5-8% slower too).
     constexpr bool kBig = (W == 64 && H <= 64 && !(H == 64 && MODE == LM_INV)) ||
                           (W == 128 && H <= 32 && MODE != LM_RT);
     // Forward / inverse tiles of 128-point register columns and 8..32 columns hold one CTA per SM
