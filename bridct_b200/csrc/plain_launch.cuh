@@ -135,19 +135,19 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     // of 8..32 x 128 (all rows busy, but no register prefetch at that size): -20%.
     constexpr bool kWide = H == 128 && W <= 32 && MODE != LM_RT;
     constexpr int TR = kWide ? Gm::kTRWide : kBig ? Gm::kTRBig : Gm::kTR;
-    constexpr int smem = kWide ? Gm::kSmemFullWide : kBig ? Gm::kSmemFullBig : Gm::kSmemFull;
     // 128 x 128 tiles (both passes 128-point register lines, 255 registers) and round trips of
     // tiles with a 128-point axis run 128-thread CTAs: two CTAs share an SM (128 x 128 +31..64%
     // over one 256-thread CTA with register prefetch, in which half the warps have no line; the
     // round trips +3..30% together with their register lines).  Forward / inverse tiles that mix
     // 128-point register lines with many short lines measured 5..13% slower that way.
     constexpr int T = (H == 128 && W == 128) || (MODE == LM_RT && (H == 128 || W == 128)) ? 128 : kThreads;
+    constexpr int smem = Gm::template tile_smem<MODE, T>(TR / H);
     if constexpr (Gm::kTRSmall < TR && small_batch_tiles(H, W, MODE)) {
       if (batch * H * W <= kSmallBatchFloats) {
         constexpr bool k64 = H == 64 && W == 64;   // two arrays, 128 threads (see small_batch_tiles)
         constexpr int TS = k64 ? 128 : T;
         constexpr int TRS = k64 ? Gm::kTR : Gm::kTRSmall;
-        constexpr int SMS = k64 ? Gm::kSmemFull : Gm::kSmemFullSmall;
+        constexpr int SMS = Gm::template tile_smem<MODE, TS>(TRS / H);
         auto ks = k_full<H, W, TRS, true, true, MODE, TS, GEN>;
         TileArgs a{x, y, (batch * H + TRS - 1) / TRS, batch * H, tab, lx, ly};
         return launch_tiles(ks, SMS, kernel_blocks_per_sm(ks, SMS, TS), a, ctx, st, TS);

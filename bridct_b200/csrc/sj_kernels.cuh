@@ -345,14 +345,19 @@ __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
   // whole-array tiles: arrays of H rows, AP floats apart (tile_array_pitch); row blocks: rows P apart
   constexpr int AH = DO_COL ? H : 1;
   constexpr int AP = DO_COL ? tile_array_pitch(H, W, P) : P;
-  constexpr int XB = (THREADS / 32) * cmax(DO_COL ? ExchangeFloats<H>::value : 0, DO_ROW ? ExchangeFloats<W>::value : 0);
+  // Only four-step lines use the exchange buffer and the staged tables; register lines (N up to
+  // the pass's reg_line_max) need neither, and the tile launches size shared memory the same way
+  // (Geometry::tile_smem).
+  constexpr bool kFsCol = DO_COL && H > reg_line_max(H, W, MODE, false);
+  constexpr bool kFsRow = DO_ROW && W > reg_line_max(W, H, MODE, !DO_COL);
+  constexpr int XB = (THREADS / 32) * cmax(kFsCol ? ExchangeFloats<H>::value : 0, kFsRow ? ExchangeFloats<W>::value : 0);
   extern __shared__ float smem[];
   float* tile = smem;
   float* xbuf = smem + round4((TR / AH) * AP);
   float* tabs = xbuf + round4(XB);
   griddep_wait();
-  const FourStepTables tcol = DO_COL ? stage_tables<H>(a.tab.col, tabs) : a.tab.col;
-  const FourStepTables trow = DO_ROW ? stage_tables<W>(a.tab.row, tabs + (DO_COL ? TableFloats<H>::value : 0))
+  const FourStepTables tcol = kFsCol ? stage_tables<H>(a.tab.col, tabs) : a.tab.col;
+  const FourStepTables trow = kFsRow ? stage_tables<W>(a.tab.row, tabs + (kFsCol ? TableFloats<H>::value : 0))
                                      : a.tab.row;
   // The last tile of a launch may hold fewer than TR rows; it is zero-filled.
   auto rows_of = [&](long long t) {
@@ -544,6 +549,15 @@ struct Geometry {
   static constexpr int full_smem(int arrays) {
     return (round4(arrays * tile_array_pitch(H, W, pitch_of(H, W, true))) + round4(kXbufFull) + TableFloats<H>::value +
             TableFloats<W>::value) * 4;
+  }
+  // Shared memory of a whole-array tile kernel (k_full<H, W, arrays * H, 1, 1, MODE, THREADS>):
+  // the tile, and for the axes whose lines run the four-step their exchange buffer and tables.
+  template <int MODE, int THREADS>
+  static constexpr int tile_smem(int arrays) {
+    constexpr bool fc = H > reg_line_max(H, W, MODE, false), fr = W > reg_line_max(W, H, MODE, false);
+    return (round4(arrays * tile_array_pitch(H, W, pitch_of(H, W, true))) +
+            round4((THREADS / 32) * cmax(fc ? ExchangeFloats<H>::value : 0, fr ? ExchangeFloats<W>::value : 0)) +
+            (fc ? TableFloats<H>::value : 0) + (fr ? TableFloats<W>::value : 0)) * 4;
   }
   static constexpr int pick_arrays(int target, int cap = kSmemTwoPerSM) {
     int a = cmax(1, target / (H * W));
