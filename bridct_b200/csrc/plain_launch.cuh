@@ -141,7 +141,9 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     // round trips +3..30% together with their register lines).  Forward / inverse tiles that mix
     // 128-point register lines with many short lines measured 5..13% slower that way.
     constexpr int T = (H == 128 && W == 128) || (MODE == LM_RT && (H == 128 || W == 128)) ? 128 : kThreads;
-    constexpr int smem = Gm::template tile_smem<MODE, T>(TR / H);
+    // Shared memory as the kernel uses it (no exchange buffer for register lines), except the
+    // 128 x 128 round trip, which measured 2-3% faster at two CTAs per SM than at three.
+    constexpr int smem = H == 128 && W == 128 && MODE == LM_RT ? Gm::kSmemFull : Gm::template tile_smem<MODE, T>(TR / H);
     if constexpr (Gm::kTRSmall < TR && small_batch_tiles(H, W, MODE)) {
       if (batch * H * W <= kSmallBatchFloats) {
         constexpr bool k64 = H == 64 && W == 64;   // two arrays, 128 threads (see small_batch_tiles)
@@ -172,10 +174,14 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     // CTA with prefetch; forward and inverse measured 5..9% slower that way and keep 256 threads.
     constexpr int TC_T = H == 128 && MODE == LM_RT ? 128 : kThreads;
     constexpr int TR_T = W == 128 && MODE == LM_RT ? 128 : kThreads;
+    constexpr int kSmemC = Gm::template strip_smem_used<MODE, TC_T>(Gm::kTC);
+    constexpr int kSmemCs = Gm::template strip_smem_used<MODE, TC_T>(Gm::kTCs);
+    constexpr int kSmemR = Gm::template rows_smem_used<MODE, TR_T>(Gm::kRB);
+    constexpr int kSmemRs = Gm::template rows_smem_used<MODE, TR_T>(Gm::kRBs);
     auto kc = k_colstrip<H, W, Gm::kTC, MODE, TC_T, GEN>;
     auto kr = k_full<H, W, Gm::kRB, false, true, MODE, TR_T, GEN>;
-    const int bpc = kernel_blocks_per_sm(kc, Gm::kSmemStrip, TC_T);
-    const int bpr = kernel_blocks_per_sm(kr, Gm::kSmemRows, TR_T);
+    const int bpc = kernel_blocks_per_sm(kc, kSmemC, TC_T);
+    const int bpr = kernel_blocks_per_sm(kr, kSmemR, TR_T);
     // One column-strip launch and one row-block launch over the whole batch.  Cutting the batch
     // into L2-sized chunks (so that the intermediate stays in L2 between the two passes) measured
     // slower on every two-pass shape: the four-step kernels are bound by shared-memory latency,
@@ -188,11 +194,11 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     if (small) {   // few arrays (or asked for): smaller strips and row blocks
       auto kcs = k_colstrip<H, W, Gm::kTCs, MODE, TC_T, GEN>;
       TileArgs ac{x, y, nb * (W / Gm::kTCs), nb * H, tab, lx, ly};
-      e = launch_tiles(kcs, Gm::kSmemStripS, kernel_blocks_per_sm(kcs, Gm::kSmemStripS, TC_T), ac, ctx, st, TC_T,
+      e = launch_tiles(kcs, kSmemCs, kernel_blocks_per_sm(kcs, kSmemCs, TC_T), ac, ctx, st, TC_T,
                        few);
     } else {
       TileArgs ac{x, y, nb * (W / Gm::kTC), nb * H, tab, lx, ly};
-      e = launch_tiles(kc, Gm::kSmemStrip, bpc, ac, ctx, st, TC_T, false);
+      e = launch_tiles(kc, kSmemC, bpc, ac, ctx, st, TC_T, false);
     }
     if (e != cudaSuccess) return e;
     if constexpr (Gm::kNarrowRows) {
@@ -202,11 +208,11 @@ cudaError_t launch_plain_impl(const float* x, float* y, long long batch, cudaStr
     } else if (nb * H / Gm::kRB < 2LL * ctx.sm_count || (GEN && lx.small_units)) {
       auto krs = k_full<H, W, Gm::kRBs, false, true, MODE, TR_T, GEN>;
       TileArgs ar{y, y, nb * H / Gm::kRBs, nb * H, tab, ly, ly};
-      e = launch_tiles(krs, Gm::kSmemRowsS, kernel_blocks_per_sm(krs, Gm::kSmemRowsS, TR_T), ar, ctx, st, TR_T,
+      e = launch_tiles(krs, kSmemRs, kernel_blocks_per_sm(krs, kSmemRs, TR_T), ar, ctx, st, TR_T,
                        few);
     } else {
       TileArgs ar{y, y, nb * H / Gm::kRB, nb * H, tab, ly, ly};
-      e = launch_tiles(kr, Gm::kSmemRows, bpr, ar, ctx, st, TR_T, false);
+      e = launch_tiles(kr, kSmemR, bpr, ar, ctx, st, TR_T, false);
     }
     if (e != cudaSuccess) return e;
     return cudaSuccess;

@@ -459,7 +459,10 @@ __global__ void __launch_bounds__(THREADS) k_colstrip(TileArgs a) {
   float* tile = smem;
   float* xbuf = smem + round4(kT ? TC * P : H * P);
   griddep_wait();
-  const FourStepTables tcol = stage_tables<H>(a.tab.col, xbuf + round4((THREADS / 32) * ExchangeFloats<H>::value));
+  // register lines (128-point columns of the two-pass shapes) need no exchange buffer or tables
+  constexpr bool kFs = H > reg_line_max(H, W, MODE, true);
+  const FourStepTables tcol =
+      kFs ? stage_tables<H>(a.tab.col, xbuf + round4((THREADS / 32) * ExchangeFloats<H>::value)) : a.tab.col;
   // Strips of 128- and 256-point columns prefetch the next strip into registers during the
   // transform; longer columns keep their occupancy.  (256-point strips of 16 columns in 128-thread
   // CTAs, five per SM but without the prefetch, measured 20-25% slower.)
@@ -607,6 +610,18 @@ struct Geometry {
   static constexpr int kSmemStrip = strip_smem(kTC);
   static constexpr int rows_smem(int rb) {
     return (round4(rb * rowblock_pitch(W)) + round4(kWarps * ExchangeFloats<W>::value) + TableFloats<W>::value) * 4;
+  }
+  // What the two-pass kernels of one mode and thread count use: the exchange buffer and tables only
+  // where the pass's lines run the four-step (strip_smem / rows_smem size the geometry).
+  template <int MODE, int THREADS>
+  static constexpr int strip_smem_used(int tc) {
+    constexpr bool fs = H > reg_line_max(H, W, MODE, true);
+    return (round4(strip_tile(tc)) + (fs ? round4((THREADS / 32) * ExchangeFloats<H>::value) + TableFloats<H>::value : 0)) * 4;
+  }
+  template <int MODE, int THREADS>
+  static constexpr int rows_smem_used(int rb) {
+    constexpr bool fs = W > reg_line_max(W, H, MODE, true);
+    return (round4(rb * rowblock_pitch(W)) + (fs ? round4((THREADS / 32) * ExchangeFloats<W>::value) + TableFloats<W>::value : 0)) * 4;
   }
   static constexpr int pick_rb() {
     int rb = cmax(1, 16384 / W);
