@@ -203,6 +203,23 @@ def test_two_pass_geometries_agree_bitwise(shape, big):
         assert torch.equal(y_batch[:1], y_one), (shape, mode)
 
 
+@pytest.mark.parametrize("shape", [(8, 16), (8, 32), (8, 64), (16, 8), (16, 16), (16, 32), (16, 64), (32, 16),
+                                   (32, 32), (32, 64), (64, 8), (64, 64)])
+def test_tile_geometries_agree_bitwise(shape):
+    # Batches up to 16 MiB of these shapes run smaller tiles (and 64x64 round trips 128-thread
+    # CTAs) than larger batches; every line runs the same register program either way, so a
+    # 20 MiB batch and three of its arrays alone agree bit for bit, in every mode.
+    h, w = shape
+    x = torch.randn((20 << 20) // (4 * h * w), h, w, device="cuda")
+    for mode in range(3):
+        y_batch = torch_api.apply(x, mode)
+        y_few = torch_api.apply(x[:3].clone(), mode)
+        torch.cuda.synchronize()
+        assert torch.equal(y_batch[:3], y_few), (shape, mode)
+    y = torch_api.apply(x[:64], 0).cpu().numpy()
+    assert O.rel_max_error(y, O.fp64_apply(x[:64].cpu().numpy(), 0), x[:64].cpu().numpy(), output_scaled=True) <= TOL
+
+
 @pytest.mark.parametrize("n", [8, 16])
 def test_impulse_basis(n):
     # every unit impulse of an n x n array (the reference's impulse-basis tests): each output is
