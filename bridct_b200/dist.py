@@ -15,6 +15,7 @@ arrays, so that ranks get equal work whatever the mix:
 
     first, count = ragged_shard_range([h * w for h, w, _ in items], rank, world)
     my_items, x_mine, first = ragged_shard(items, x_packed, rank, world)   # a slice of the buffer
+    y = apply_ragged_sharded(items, x_packed, devices=[0, 1])            # one process, two GPUs
 """
 from __future__ import annotations
 
@@ -63,6 +64,57 @@ def ragged_shard(items: Sequence[Tuple[int, int, int]], x, rank: int, world: int
     start = sum(sizes[:first])
     end = start + sum(sizes[first:first + count])
     return list(items[first:first + count]), x[start:end], first
+
+
+def apply_ragged_sharded(items: Sequence[Tuple[int, int, int]], x, devices: Optional[Sequence[int]] = None,
+                         transform: Optional[Callable] = None):
+    """Transforms a ragged batch packed back to back in x (a flat float32 tensor or numpy array)
+    split over several GPUs of this process by elements (ragged_shard): share i goes to devices[i]
+    as its own RaggedBatch on that device's current stream, and the results come back in order,
+    packed like x (a tensor on x's device, or a numpy array).  No collective is involved.
+
+    `transform(items, piece, device)` replaces the per-device transform."""
+    import numpy as np
+
+    if devices is None:
+        import torch
+
+        devices = list(range(torch.cuda.device_count()))
+    if not devices:
+        raise ValueError("apply_ragged_sharded needs at least one device")
+    if transform is None:
+        transform = _ragged_device_transform
+    world = len(devices)
+    outs: List[Tuple[int, object]] = []
+    for r, dev in enumerate(devices):
+        mine, piece, first = ragged_shard(items, x, r, world)
+        if mine:
+            outs.append((first, mine, transform(mine, piece, dev)))
+    pos = 0
+    for first, mine, y in outs:                     # the shares tile the batch in order
+        if first != pos:
+            raise ValueError(f"ragged shares do not tile the batch: expected item {pos}, got {first}")
+        pos += len(mine)
+    if pos != len(items):
+        raise ValueError(f"ragged shares cover {pos} of {len(items)} arrays")
+    pieces = [y for _, _, y in outs]
+    if isinstance(x, np.ndarray):
+        return np.concatenate([np.asarray(p.cpu() if hasattr(p, "cpu") else p) for p in pieces]) if pieces \
+            else np.zeros(0, np.float32)
+    import torch
+
+    return torch.cat([p.to(x.device) for p in pieces]) if pieces else x.new_empty(0)
+
+
+def _ragged_device_transform(items, piece, dev):
+    import numpy as np
+    import torch
+
+    from .ragged import RaggedBatch
+
+    t = torch.from_numpy(np.ascontiguousarray(piece)) if isinstance(piece, np.ndarray) else piece
+    with torch.cuda.device(dev):
+        return RaggedBatch(items).apply(t.to(f"cuda:{dev}", non_blocking=True).contiguous())
 
 
 def shard(x, rank: int, world: int):

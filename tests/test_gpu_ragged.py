@@ -314,3 +314,18 @@ def test_launch_count_matches_the_kernels_one_apply_runs():
                    and "memset" not in e.name.lower() and "memcpy" not in e.name.lower()]
         assert len(kernels) == batch.launch_count(), sorted(e.name for e in kernels)
     assert m.launch_count() > 1
+
+
+def test_apply_ragged_sharded_matches_one_batch():
+    """The element split over the GPUs of one process (here device 0 twice) gives the single
+    batch's results bit for bit: each array is transformed by the same kernels either way."""
+    from bridct_b200.dist import apply_ragged_sharded
+
+    items = random_batch(90, 41)
+    b = RaggedBatch(items)
+    x = torch.from_numpy(np.random.default_rng(42).uniform(-1, 1, b.span).astype(np.float32)).cuda()
+    y_one = b.apply(x)
+    y_split = apply_ragged_sharded(items, x, devices=[0, 0])
+    torch.cuda.synchronize()
+    assert y_split.device == x.device and y_split.shape == x.shape
+    assert torch.equal(y_split, y_one)

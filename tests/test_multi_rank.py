@@ -197,3 +197,31 @@ def test_two_gloo_ranks_transform_balanced_ragged_shards():
     status, same, counts = q.get(timeout=10)
     assert status == "ok" and same, (status, same)
     assert sum(counts) == 41 and min(counts) > 0
+
+
+def test_apply_ragged_sharded_partition_logic_on_cpu():
+    """apply_ragged_sharded's element split and in-order stitch, with the oracle as each device's
+    transform (per array)."""
+    from bridct_b200.dist import apply_ragged_sharded
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(21)
+    items = [(int(2 ** rng.integers(3, 7)), int(2 ** rng.integers(3, 7)), int(rng.integers(0, 3))) for _ in range(29)]
+    x = rng.uniform(-1, 1, sum(h * w for h, w, _ in items)).astype(np.float32)
+    seen = []
+
+    def fake(mine, piece, dev):
+        seen.append((dev, len(mine)))
+        out, pos = [], 0
+        for h, w, m in mine:
+            out.append(O.sj_apply(piece[pos:pos + h * w].reshape(1, h, w), m).ravel())
+            pos += h * w
+        return np.concatenate(out)
+
+    y = apply_ragged_sharded(items, x, devices=[0, 1, 2], transform=fake)
+    assert [d for d, _ in seen] == [0, 1, 2] and sum(n for _, n in seen) == 29
+    pos, want = 0, []
+    for h, w, m in items:
+        want.append(O.sj_apply(x[pos:pos + h * w].reshape(1, h, w), m).ravel())
+        pos += h * w
+    assert np.array_equal(y, np.concatenate(want))
