@@ -126,6 +126,14 @@ __host__ __device__ constexpr int strip_pitch(int h, int tc) {
   return h == 256 || (h == 512 && tc == 32) ? tc + 2 : pitch_of(h, tc, true);
 }
 __host__ __device__ constexpr int rowblock_pitch(int w) { return w == 256 ? w + 8 : w == 512 ? w + 16 : w + 4; }
+// Row pitch of a whole-array tile.  Where one axis runs the four-step and the other register lines,
+// the four-step axis takes the two-pass kernels' bank-model pitch: 256-point columns w + 2, 256- and
+// 512-point rows w + 8 and w + 16 (per line group 142, 174 and 190 wavefronts against 206, 270 and
+// 222 at w + 4; tests/test_bank_model.py).  Shapes with four-step lines on both axes (256 x 128,
+// 128 x 256) keep w + 4, which the model counts as good or better for the two walks together.
+__host__ __device__ constexpr int tile_pitch(int h, int w) {
+  return h == 256 && w <= 64 ? w + 2 : w == 256 && h <= 64 ? w + 8 : w == 512 && h <= 64 ? w + 16 : pitch_of(h, w, true);
+}
 // Array pitch in a whole-array tile.  With pitch w + 4, h * (w + 4) is a multiple of 32 floats for
 // every shape, so the register-line column walks of the 4 (w = 8) or 2 (w = 16) arrays that a
 // warp's 32 lines span share banks (4- and 2-way conflicts; the tile kernel of 32 x 8 arrays spent
@@ -341,7 +349,7 @@ template <int H, int W, int TR, bool DO_COL, bool DO_ROW, int MODE, int THREADS 
           bool UNITS = false>
 __global__ void __launch_bounds__(THREADS) k_full(TileArgs a) {
   static_assert(!UNITS || !DO_COL, "merged units are row blocks");
-  constexpr int P = DO_COL ? pitch_of(H, W, true) : rowblock_pitch(W);
+  constexpr int P = DO_COL ? tile_pitch(H, W) : rowblock_pitch(W);
   // whole-array tiles: arrays of H rows, AP floats apart (tile_array_pitch); row blocks: rows P apart
   constexpr int AH = DO_COL ? H : 1;
   constexpr int AP = DO_COL ? tile_array_pitch(H, W, P) : P;
@@ -550,7 +558,7 @@ struct Geometry {
   // tile class
   static constexpr int kXbufFull = kWarps * cmax(ExchangeFloats<H>::value, ExchangeFloats<W>::value);
   static constexpr int full_smem(int arrays) {
-    return (round4(arrays * tile_array_pitch(H, W, pitch_of(H, W, true))) + round4(kXbufFull) + TableFloats<H>::value +
+    return (round4(arrays * tile_array_pitch(H, W, tile_pitch(H, W))) + round4(kXbufFull) + TableFloats<H>::value +
             TableFloats<W>::value) * 4;
   }
   // Shared memory of a whole-array tile kernel (k_full<H, W, arrays * H, 1, 1, MODE, THREADS>):
@@ -558,7 +566,7 @@ struct Geometry {
   template <int MODE, int THREADS>
   static constexpr int tile_smem(int arrays) {
     constexpr bool fc = H > reg_line_max(H, W, MODE, false), fr = W > reg_line_max(W, H, MODE, false);
-    return (round4(arrays * tile_array_pitch(H, W, pitch_of(H, W, true))) +
+    return (round4(arrays * tile_array_pitch(H, W, tile_pitch(H, W))) +
             round4((THREADS / 32) * cmax(fc ? ExchangeFloats<H>::value : 0, fr ? ExchangeFloats<W>::value : 0)) +
             (fc ? TableFloats<H>::value : 0) + (fr ? TableFloats<W>::value : 0)) * 4;
   }

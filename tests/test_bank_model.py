@@ -201,3 +201,17 @@ def test_padded_arrays_make_narrow_tile_columns_conflict_free():
         padded = sum(wavefronts([(l // w) * ap + i * p + l % w for l in range(32)]) for i in range(h))
         assert padded == h, (h, w)
         assert plain == h * 32 // w, (h, w)                  # 4-way (w = 8), 2-way (w = 16) before
+
+
+def test_tile_pitches_of_four_step_axes_beside_register_lines():
+    """Whole-array tiles whose one axis runs the four-step and the other register lines take the
+    two-pass kernels' pitches for the four-step axis (tile_pitch in sj_kernels.cuh): 256-point
+    columns w + 2, 256- and 512-point rows w + 8 and w + 16.  Where both axes run the four-step
+    (256 x 128, 128 x 256) w + 4 is as good or better for the two walks together."""
+    for w in (8, 16, 32, 64):
+        assert four_step_wavefronts(8, w + 2, rows=False) < 0.75 * four_step_wavefronts(8, w + 4, rows=False)
+    assert four_step_wavefronts(8, 264, rows=True) < 0.7 * four_step_wavefronts(8, 260, rows=True)
+    assert four_step_wavefronts(16, 528, rows=True) < 0.9 * four_step_wavefronts(16, 516, rows=True)
+    both = lambda p, gc, gr: four_step_wavefronts(gc, p, rows=False) + four_step_wavefronts(gr, p, rows=True)
+    assert both(132, 8, 4) < both(130, 8, 4)          # 256 x 128
+    assert both(260, 4, 8) <= both(264, 4, 8)         # 128 x 256
